@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Benchmark: atoms/s of the Matching Pursuit decomposition on B200.
+
+Workload (the reference's headline multichannel configuration): MMP2,
+19 channels x 8 epochs x 5120 float32 samples at 256 Hz, energyError 0.01,
+100 iterations, energyPercent 99, seeded synthetic signals (20 shared Gabor
+atoms per epoch with N(0,1) channel gains, white noise at 5 dB per channel).
+One step = the whole decomposition of the 8 epochs (800 MP atoms) as one
+device batch.  An MMP2 multichannel atom counts once.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU: one process per GPU (torchrun); each rank decomposes its own
+8-epoch workload (weak scaling, no data-path collective); the timed region is
+bracketed by a barrier and synchronize, and the max over ranks is reported.
+
+--impl reference times the reference's own CPU code (empi's src/*.cpp built
+by oracle/Makefile with the project FFT shim in place of FFTW) on one epoch
+of the same workload per step, on rank 0 with all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = 1  # empi_b200.synth workload index
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    return rank, local, world
+
+
+# ---------------------------------------------------------------- reference arm
+
+
+def reference_config(d, w, epoch_index, iterations):
+    path = os.path.join(d, "sig.bin")
+    w.epochs[epoch_index].tofile(path)
+    cfg = os.path.join(d, "cfg")
+    with open(cfg, "w") as f:
+        f.write(f"energyError {w.energy_error}\nmaximalNumberOfIterations {iterations}\n"
+                f"energyPercent {w.energy_percent}\nMP {w.variant.upper()}\nnameOfDataFile sig.bin\n"
+                f"nameOfOutputDirectory .\nsamplingFrequency {w.fs}\nnumberOfChannels {w.channels}\n"
+                f"selectedChannels 1-{w.channels}\nnumberOfSamplesInEpoch {w.samples}\n")
+    return cfg
+
+
+def run_reference(w, iterations, threads):
+    """Wall time and atom count of the reference CLI on epoch 0."""
+    from oracle import oracle as O
+
+    cli = O.ref_cli()
+    if not os.path.exists(cli):
+        return None
+    with tempfile.TemporaryDirectory() as d:
+        cfg = reference_config(d, w, 0, iterations)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close")
+        t0 = time.perf_counter()
+        p = subprocess.run([cli, cfg], cwd=d, env=env, capture_output=True, text=True, check=True)
+        dt = time.perf_counter() - t0
+    atoms = sum(1 for line in p.stdout.splitlines() if line.startswith("ATOM"))
+    return dt, atoms
+
+
+def reference_arm(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return
+    from empi_b200 import synth
+
+    w = synth.workload(WORKLOAD)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        r = run_reference(w, 5, threads)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/empi not built (make -C oracle ref)"}))
+            return
+    times, atoms = [], 0
+    for _ in range(args.steps):
+        dt, n = run_reference(w, w.iterations, threads)
+        times.append(dt)
+        atoms += n
+    total = sum(times)
+    value = atoms / total
+    sample = (f"epoch 0 of the workload per step ({w.channels}ch x {w.samples} @ {w.fs:g} Hz, "
+              f"{w.variant.upper()}, {w.iterations} iterations), reference CLI built from empi src/*.cpp "
+              f"-O3 -fopenmp with the project FP64 FFT shim (FFTW absent)")
+    line = {
+        "impl": "reference", "metric": "atoms/s", "value": value, "unit": "atoms/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config(w, world),
+        "cpu_baseline": {"value": value, "unit": "atoms/s", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "atoms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def workload_config(w, world):
+    return {"workload": f"{w.variant.upper()} {w.channels}ch x {len(w.epochs)} epochs x {w.samples} "
+                        f"float32 @ {w.fs:g} Hz, energyError {w.energy_error}, {w.iterations} iterations, "
+                        f"energyPercent {w.energy_percent}",
+            "variant": w.variant, "channels": w.channels, "epochs": len(w.epochs), "samples": w.samples,
+            "fs": w.fs, "energy_error": w.energy_error, "iterations": w.iterations,
+            "energy_percent": w.energy_percent, "parallelism": f"instances x{world} (weak)",
+            "l2": "256 MiB buffer written between timed steps (inputs are smaller than L2)"}
+
+
+# ---------------------------------------------------------------- clocks
+
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "-i", str(self.device),
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=self.file, stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- our arm
+
+
+def cpu_baseline(w):
+    threads = os.cpu_count() or 1
+    r = run_reference(w, w.iterations, threads)
+    if r is None:
+        return None
+    dt, atoms = r
+    return {"value": atoms / dt, "unit": "atoms/s", "cores": threads, "kind": "reference",
+            "sample": f"epoch 0 of the workload ({w.channels}ch x {w.samples} @ {w.fs:g} Hz, "
+                      f"{w.variant.upper()}, {w.iterations} iterations, {dt:.2f} s), reference CLI from "
+                      f"empi src/*.cpp -O3 -fopenmp with the project FP64 FFT shim (FFTW absent)"}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def profiled_traffic():
+    """dram bytes per refresh launch from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "refresh_traffic.json")) as f:
+            return json.load(f)
+    except OSError:
+        return None
+
+
+def ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import empi_b200
+    from empi_b200 import synth
+
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    w = synth.workload(WORKLOAD, seed=1000 + WORKLOAD + 7919 * rank)
+    stream = torch.cuda.Stream()
+    eng = empi_b200.Engine(device=local, stream=stream.cuda_stream)
+    settings = empi_b200.DecompositionSettings(w.iterations, 1.0 - 0.01 * w.energy_percent)
+    shapes = [e.shape for e in w.epochs]
+    pinned = [torch.from_numpy(e).pin_memory() for e in w.epochs]
+    host = [p.numpy() for p in pinned]
+    batch = empi_b200.Batch(w.variant, w.energy_error, settings, shapes, w.fs, engine=eng)
+    batch.load(host)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
+
+    def atoms_of():
+        return sum(int(batch.result(e).counts[0]) if w.variant != "smp" else int(batch.result(e).counts.sum())
+                   for e in range(len(w.epochs)))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        batch.run()
+    atoms_per_step = atoms_of()
+
+    # device-resident inputs: one step = batch.run()
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        batch.run()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    barrier()
+    clk = clocks.stop()
+    launches = batch.stats().kernel_launches
+
+    # end to end through the public API: pinned host inputs in, atoms out
+    e2e_ms = 0.0
+    d2h = 0
+    barrier()
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        batch.load(host)
+        batch.run()
+        d2h = 0
+        for e in range(len(w.epochs)):
+            r = batch.result(e)
+            d2h += r.atoms.nbytes + r.counts.nbytes + r.energies.nbytes + r.indices.nbytes + r.totals.nbytes
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+    barrier()
+    h2d = sum(e.nbytes for e in host)
+
+    t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms, e2e_ms = float(t[0]), float(t[1])
+    units = atoms_per_step * args.steps * world
+    value = units / (total_ms / 1e3)
+    e2e_value = units / (e2e_ms / 1e3)
+
+    # dominant kernel (k_refresh): CUDA events around every refresh launch
+    eng_t = empi_b200.Engine(device=local, stream=stream.cuda_stream, timing=True)
+    bt = empi_b200.Batch(w.variant, w.energy_error, settings, shapes, w.fs, engine=eng_t)
+    bt.load(host)
+    bt.run()
+    bt.run()
+    st = bt.stats()
+    per_launch_ms = st.refresh_ms / max(1, st.refresh_launches)
+    bytes_per_launch = st.algorithmic_bytes / max(1, st.refresh_launches)
+    flops_per_launch = st.fft_flops / max(1, st.refresh_launches)
+    peaks, peak_kind = measured_peaks()
+    achieved_gbs = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
+    tr = profiled_traffic()
+    roofline = {"kernel": "k_refresh (windowed FFT + energy + slot max)", "bound": "hbm",
+                "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved_gbs / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs",
+                "traffic": tr.get("dram_bytes_per_launch") if tr else None,
+                "launch_ms": per_launch_ms, "launches": st.refresh_launches,
+                "algorithmic_bytes_per_launch": bytes_per_launch}
+    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
+    roofline_fp32 = {"achieved": flops_per_launch / (per_launch_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+                     "peak": fp32_peak, "peak_source": "nominal FP32 CUDA-core (148 SMs x 128 x 2 x 1.965 GHz)",
+                     "frac": flops_per_launch / (per_launch_ms * 1e-3) / 1e12 / fp32_peak,
+                     "flops": "reference-equivalent 2.5 Nfft log2 Nfft per refreshed window"}
+    bt.close()
+    eng_t.close()
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(w)
+    if rank == 0:
+        line = {
+            "metric": "atoms/s", "value": value, "unit": "atoms/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FFT maps) + f64 (rescore, residual, energies)",
+            "data": "synthetic", "config": workload_config(w, world),
+            "e2e": {"value": e2e_value, "unit": "atoms/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches, "roofline": roofline, "roofline_fp32": roofline_fp32,
+            "cpu_baseline": base, "clocks": clk, "atoms_per_step": atoms_per_step,
+            "candidate_bins_per_atom": st.candidate_bins / max(1, st.atoms),
+        }
+        print(json.dumps(line))
+    batch.close()
+    eng.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,80 @@
+"""Builds the sm_100a engine in-tree: empi_b200/libempi_b200.so and the
+empi-gpu CLI (empi_b200/empi-gpu).
+
+    python -m empi_b200.build [--force]
+
+nvcc cross-compiles for sm_100a without a GPU.  The CUDA runtime is linked
+statically so the library loads without extra library paths.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libempi_b200.so")
+CLI = os.path.join(HERE, "empi-gpu")
+BUILD = os.path.join(HERE, "_build")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+                     "--expt-relaxed-constexpr", "-diag-suppress", "177"]
+SOURCES = ["engine.cu", "geometry.cpp", "hostio.cpp"]
+HEADERS = ["fft.cuh", "kernels.cuh", "plan.hpp", "geometry.hpp", "engine.hpp"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def host_cxx() -> str:
+    return "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+
+
+def _newest(paths):
+    return max(os.path.getmtime(p) for p in paths if os.path.exists(p))
+
+
+def _stale(target, deps) -> bool:
+    return not os.path.exists(target) or os.path.getmtime(target) < _newest(deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [
+        os.path.join(ROOT, "include", "empi_b200.h"), __file__]
+    os.makedirs(BUILD, exist_ok=True)
+    cc = nvcc()
+    ccbin = ["-ccbin", host_cxx()]
+    if force or _stale(LIB, deps):
+        objs = []
+        for src in SOURCES:
+            obj = os.path.join(BUILD, src + ".o")
+            cmd = [cc] + ccbin + NVCC_FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
+            if src.endswith(".cpp"):
+                cmd = [cc] + ccbin + ["-x", "cu"] + NVCC_FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.run(cmd, check=True)
+            objs.append(obj)
+        tmp = LIB + ".tmp"
+        cmd = [cc] + ccbin + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, LIB)
+    cli_src = os.path.join(CSRC, "empi_cli.cpp")
+    if force or _stale(CLI, [cli_src, LIB]):
+        cmd = [host_cxx(), "-O2", "-std=c++17", "-o", CLI, cli_src, "-L" + HERE, "-lempi_b200",
+               "-Wl,-rpath,$ORIGIN"]
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    print(LIB)

@@ -1,0 +1,939 @@
+// Host engine: device state of batches and workspaces, CUDA-graph capture of
+// the MP iteration, and the C ABI declared in include/empi_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/empi_b200.h"
+#include "engine.hpp"
+#include "geometry.hpp"
+#include "kernels.cuh"
+
+using namespace empi;
+
+// ------------------------------------------------------------ errors
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+namespace empi {
+
+empi_status fail(empi_status st, const std::string& msg) {
+    g_last_error = msg;
+    return st;
+}
+
+empi_status ok() {
+    g_last_error.clear();
+    return EMPI_OK;
+}
+
+}  // namespace empi
+
+#define CUDA_TRY(expr)                                                                     \
+    do {                                                                                   \
+        cudaError_t e_ = (expr);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            return fail(e_ == cudaErrorMemoryAllocation ? EMPI_ERR_OUT_OF_MEMORY : EMPI_ERR_CUDA, \
+                        e_ == cudaErrorMemoryAllocation ? std::string("insufficientMemory")  \
+                                                        : std::string("cuda: ") + cudaGetErrorString(e_)); \
+        }                                                                                  \
+    } while (0)
+
+extern "C" const char* empi_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int empi_abi_version(void) { return EMPI_B200_ABI_VERSION; }
+
+extern "C" const char* empi_status_string(empi_status st) {
+    switch (st) {
+        case EMPI_OK: return "ok";
+        case EMPI_ERR_INVALID_ARGUMENT: return "invalidArgument";
+        case EMPI_ERR_CUDA: return "cudaError";
+        case EMPI_ERR_OUT_OF_MEMORY: return "insufficientMemory";
+        case EMPI_ERR_SIGNAL_IS_EMPTY: return "signalIsEmpty";
+        case EMPI_ERR_ENERGY_MAP_IS_EMPTY: return "energyMapIsEmpty";
+        case EMPI_ERR_SIGNAL_TOO_LONG: return "signalFileIsTooLongForThisDecomposition";
+        case EMPI_ERR_CANDIDATE_OVERFLOW: return "candidateOverflow";
+        case EMPI_ERR_CONFIG: return "configurationError";
+        case EMPI_ERR_IO: return "ioError";
+        case EMPI_ERR_NO_DEVICE: return "noCudaDevice";
+        case EMPI_ERR_INTERNAL: return "internalError";
+    }
+    return "unknown";
+}
+
+// ------------------------------------------------------------ engine
+
+struct empi_engine {
+    empi_engine_opts opts;
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    float2* tw = nullptr;
+};
+
+extern "C" void empi_engine_opts_default(empi_engine_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->transform_cap = 4096;
+    o->candidate_band = 1e-4;
+    o->candidate_capacity = 0;
+    o->iterations_per_graph = 8;
+}
+
+namespace {
+
+empi_status set_device(const empi_engine* e) {
+    CUDA_TRY(cudaSetDevice(e->device));
+    return EMPI_OK;
+}
+
+}  // namespace
+
+extern "C" empi_status empi_engine_create(const empi_engine_opts* opts, empi_engine** out) {
+    if (!out) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    *out = nullptr;
+    std::unique_ptr<empi_engine> e(new empi_engine);
+    empi_engine_opts_default(&e->opts);
+    if (opts) {
+        e->opts = *opts;
+        if (e->opts.transform_cap == 0) e->opts.transform_cap = 4096;
+        if (e->opts.candidate_band <= 0) e->opts.candidate_band = 1e-4;
+        if (e->opts.iterations_per_graph <= 0) e->opts.iterations_per_graph = 8;
+    }
+    int n = 0;
+    cudaError_t ce = cudaGetDeviceCount(&n);
+    if (ce != cudaSuccess || n == 0) return fail(EMPI_ERR_NO_DEVICE, "noCudaDevice");
+    e->device = e->opts.device;
+    if (e->device < 0 || e->device >= n) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidDevice");
+    CUDA_TRY(cudaSetDevice(e->device));
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, e->device));
+    if (prop.major < 10) return fail(EMPI_ERR_NO_DEVICE, "deviceIsNotSm100");
+    e->sms = prop.multiProcessorCount;
+    if (e->opts.stream) {
+        e->stream = (cudaStream_t)e->opts.stream;
+    } else {
+        CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+        e->own_stream = true;
+    }
+    std::vector<float2> tw(kTwN);
+    for (int m = 0; m < kTwN; ++m) {
+        long double a = 6.283185307179586476925286766559005768L * (long double)m / (long double)kTwN;
+        tw[m] = make_float2((float)cosl(a), (float)(-sinl(a)));
+    }
+    CUDA_TRY(cudaMalloc(&e->tw, sizeof(float2) * kTwN));
+    CUDA_TRY(cudaMemcpy(e->tw, tw.data(), sizeof(float2) * kTwN, cudaMemcpyHostToDevice));
+    *out = e.release();
+    return ok();
+}
+
+extern "C" void empi_engine_destroy(empi_engine* e) {
+    if (!e) return;
+    cudaSetDevice(e->device);
+    if (e->tw) cudaFree(e->tw);
+    if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+// ------------------------------------------------------------ dictionary queries
+
+extern "C" empi_status empi_dictionary_size(const empi_dictionary* d, double fs, int samples, uint64_t* count,
+                                            int* scales) {
+    if (!d) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    DictPlan dp;
+    std::vector<ScalePlan> sp;
+    std::string err;
+    if (!build_dictionary(fs, samples, d->energy_error, d->scale_min, d->scale_max, d->freq_max, 4096, dp, sp,
+                          err))
+        return fail(err == "signalFileIsTooLongForThisDecomposition" ? EMPI_ERR_SIGNAL_TOO_LONG
+                                                                     : EMPI_ERR_INVALID_ARGUMENT,
+                    err);
+    if (count) *count = dp.values;
+    if (scales) *scales = dp.nscales;
+    return ok();
+}
+
+extern "C" empi_status empi_dictionary_scales(const empi_dictionary* d, double fs, int samples, int cap, double* s,
+                                              int* nfft, int* fcount, int* tcount, int* count) {
+    if (!d) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    DictPlan dp;
+    std::vector<ScalePlan> sp;
+    std::string err;
+    if (!build_dictionary(fs, samples, d->energy_error, d->scale_min, d->scale_max, d->freq_max, 4096, dp, sp,
+                          err))
+        return fail(EMPI_ERR_INVALID_ARGUMENT, err);
+    for (int i = 0; i < dp.nscales && i < cap; ++i) {
+        if (s) s[i] = sp[i].s;
+        if (nfft) nfft[i] = sp[i].nfft;
+        if (fcount) fcount[i] = sp[i].fcount;
+        if (tcount) tcount[i] = sp[i].tcount;
+    }
+    if (count) *count = dp.nscales;
+    return ok();
+}
+
+// ------------------------------------------------------------ batch state
+
+namespace {
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t alloc(size_t count) {
+        n = std::max<size_t>(count, 1);
+        return cudaMalloc(&p, sizeof(T) * n);
+    }
+};
+
+}  // namespace
+
+struct empi_batch {
+    empi_engine* eng = nullptr;
+    int variant = 0, mode = MODE_SINGLE;
+    empi_settings settings{};
+    std::vector<DictPlan> dicts;
+    std::vector<ScalePlan> scales;
+    std::vector<InstPlan> insts;
+    std::vector<int2> blk_ic;
+    std::vector<int2> fit_map;      // MMP2: (instance, input channel)
+    std::vector<empi_epoch> epochs; // shapes
+    std::vector<long long> epoch_in_off;
+    std::vector<int> epoch_first_inst;
+    std::vector<int> epoch_first_fit;
+    int cmax = 1, nij = 0;
+    long long total_in = 0;
+    int max_n = 0;
+
+    DevBuf<ScalePlan> d_scales;
+    DevBuf<DictPlan> d_dicts;
+    DevBuf<InstPlan> d_insts;
+    DevBuf<int2> d_blk_ic, d_fit_map;
+    DevBuf<float> d_input;
+    DevBuf<double> d_residual, d_atoms, d_energies, d_chan_energy, d_fit_atoms, d_stats;
+    DevBuf<InstState> d_state;
+    DevBuf<unsigned long long> d_slots, d_chunks;
+    DevBuf<int2> d_dirty, d_crange;
+    DevBuf<int> d_ij_units, d_ij_chunks, d_inst_units, d_inst_chunks, d_ctr, d_inst_bins;
+    DevBuf<CandSlot> d_cslots;
+    DevBuf<CandBin> d_cbins;
+    DevBuf<double2> d_cbin_v;
+    DevBuf<int4> d_indices;
+    DevBuf<float> d_dump;
+
+    BatchDev dev{};
+    int refresh_grid = 0, collect_grid = 0, tree_grid = 0, rescore_grid = 0;
+    size_t refresh_smem = 0;
+
+    cudaGraphExec_t graph = nullptr;
+    int graph_iters = 0;
+    std::vector<cudaEvent_t> ev;  // timing pairs around refresh launches
+    int ev_used = 0;
+    cudaEvent_t run_start = nullptr, run_stop = nullptr;
+
+    empi_batch_stats stats{};
+    int launches_per_iter = 10;
+
+    ~empi_batch() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (auto e : ev) cudaEventDestroy(e);
+        if (run_start) cudaEventDestroy(run_start);
+        if (run_stop) cudaEventDestroy(run_stop);
+    }
+};
+
+namespace {
+
+template <int MODE>
+empi_status configure_refresh(empi_batch* b) {
+    const size_t smem = refresh_smem_bytes<MODE>();
+    CUDA_TRY(cudaFuncSetAttribute(k_refresh<MODE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_TRY(cudaFuncSetAttribute(k_refresh<MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_refresh<MODE, false>, kUnitThreads, smem));
+    if (occ < 1) return fail(EMPI_ERR_INTERNAL, "refreshKernelDoesNotFit");
+    b->refresh_smem = smem;
+    b->refresh_grid = b->eng->sms * occ;
+    b->collect_grid = b->eng->sms * occ;
+    return EMPI_OK;
+}
+
+empi_status configure(empi_batch* b) {
+    switch (b->mode) {
+        case MODE_SINGLE: return configure_refresh<MODE_SINGLE>(b);
+        case MODE_MMP1: return configure_refresh<MODE_MMP1>(b);
+        default: return configure_refresh<MODE_MMP3>(b);
+    }
+}
+
+void launch_refresh(empi_batch* b, bool collect, cudaStream_t s) {
+    const dim3 grid(collect ? b->collect_grid : b->refresh_grid), block(kUnitThreads);
+    switch (b->mode) {
+        case MODE_SINGLE:
+            if (collect) k_refresh<MODE_SINGLE, true><<<grid, block, b->refresh_smem, s>>>(b->dev);
+            else k_refresh<MODE_SINGLE, false><<<grid, block, b->refresh_smem, s>>>(b->dev);
+            break;
+        case MODE_MMP1:
+            if (collect) k_refresh<MODE_MMP1, true><<<grid, block, b->refresh_smem, s>>>(b->dev);
+            else k_refresh<MODE_MMP1, false><<<grid, block, b->refresh_smem, s>>>(b->dev);
+            break;
+        default:
+            if (collect) k_refresh<MODE_MMP3, true><<<grid, block, b->refresh_smem, s>>>(b->dev);
+            else k_refresh<MODE_MMP3, false><<<grid, block, b->refresh_smem, s>>>(b->dev);
+            break;
+    }
+}
+
+// schedule + refresh + tree + root (the map update after a subtraction, or
+// the initial pass)
+void launch_update(empi_batch* b, int sched_mode, int only_scale, double tA, double sA, cudaStream_t s,
+                   cudaEvent_t e0, cudaEvent_t e1) {
+    const int ninst = (int)b->insts.size();
+    k_sched_a<<<ninst, 128, 0, s>>>(b->dev, sched_mode, only_scale, tA, sA);
+    k_sched_b<<<1, 1024, 0, s>>>(b->dev);
+    if (e0) cudaEventRecord(e0, s);
+    launch_refresh(b, false, s);
+    if (e1) cudaEventRecord(e1, s);
+    k_tree<<<b->tree_grid, 256, 0, s>>>(b->dev);
+    k_root<<<ninst, 256, 0, s>>>(b->dev);
+}
+
+// candidates -> FP64 rescore -> atom
+void launch_select(empi_batch* b, cudaStream_t s) {
+    const int ninst = (int)b->insts.size();
+    k_cand_slots<<<ninst, 256, 0, s>>>(b->dev);
+    launch_refresh(b, true, s);
+    k_rescore<<<b->rescore_grid, 128, 0, s>>>(b->dev);
+    k_select<<<ninst, 128, 0, s>>>(b->dev);
+}
+
+void launch_iteration(empi_batch* b, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+    launch_select(b, s);
+    k_subtract<<<(int)b->blk_ic.size(), 256, 0, s>>>(b->dev);
+    launch_update(b, SCHED_ITERATE, -1, 0.0, 0.0, s, e0, e1);
+}
+
+empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* dict, const empi_settings* settings,
+                        const empi_epoch* epochs, int count, int result_iters, empi_batch** out) {
+    if (!eng || !dict || !epochs || count <= 0 || !out) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    if (settings && settings->iteration_max <= 0) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidMaximalNumberOfIterations");
+    if (settings && (settings->residual_energy < 0 || settings->residual_energy >= 1.0))
+        return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidEnergyPercentValue");
+    if (variant < EMPI_SMP || variant > EMPI_MMP3) return fail(EMPI_ERR_INVALID_ARGUMENT, "unsupportedDecompositionType");
+    empi_status st = set_device(eng);
+    if (st != EMPI_OK) return st;
+    std::unique_ptr<empi_batch> b(new empi_batch);
+    b->eng = eng;
+    b->variant = variant;
+    b->settings = settings ? *settings : empi_settings{result_iters, 0.0};
+    const int iters = b->settings.iteration_max;
+    std::map<std::pair<double, int>, int> dict_of;
+    bool multi = false;
+    for (int e = 0; e < count; ++e) {
+        const empi_epoch& ep = epochs[e];
+        if (ep.channels <= 0 || ep.samples <= 0) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidEpochShape");
+        if (ep.channels > kMaxChannels && (variant == EMPI_MMP1 || variant == EMPI_MMP3))
+            return fail(EMPI_ERR_INVALID_ARGUMENT, "tooManyChannels");
+        auto key = std::make_pair(ep.fs, ep.samples);
+        if (!dict_of.count(key)) {
+            DictPlan dp;
+            std::string err;
+            if (!build_dictionary(ep.fs, ep.samples, dict->energy_error, dict->scale_min, dict->scale_max,
+                                  dict->freq_max, eng->opts.transform_cap, dp, b->scales, err))
+                return fail(err == "signalFileIsTooLongForThisDecomposition" ? EMPI_ERR_SIGNAL_TOO_LONG
+                                                                             : EMPI_ERR_INVALID_ARGUMENT,
+                            err);
+            dict_of[key] = (int)b->dicts.size();
+            b->dicts.push_back(dp);
+        }
+        b->epochs.push_back(ep);
+        b->epoch_in_off.push_back(b->total_in);
+        b->total_in += (long long)ep.channels * ep.samples;
+        b->max_n = std::max(b->max_n, ep.samples);
+        if ((variant == EMPI_MMP1 || variant == EMPI_MMP3) && ep.channels > 1) multi = true;
+    }
+    b->mode = !multi ? MODE_SINGLE : (variant == EMPI_MMP1 ? MODE_MMP1 : MODE_MMP3);
+    long long res_off = 0, slot_off = 0, chunk_off = 0, out_off = 0;
+    int ij_off = 0, cen_off = 0;
+    for (int e = 0; e < count; ++e) {
+        const empi_epoch& ep = epochs[e];
+        const int d = dict_of[std::make_pair(ep.fs, ep.samples)];
+        const DictPlan& dp = b->dicts[d];
+        b->epoch_first_inst.push_back((int)b->insts.size());
+        b->epoch_first_fit.push_back((int)b->fit_map.size());
+        auto add = [&](int C, int chan0) {
+            InstPlan ip{};
+            ip.dict = d;
+            ip.C = C;
+            ip.epoch = e;
+            ip.chan0 = chan0;
+            ip.ij_off = ij_off;
+            ip.cen_off = cen_off;
+            ip.res_off = res_off;
+            ip.slot_off = slot_off;
+            ip.chunk_off = chunk_off;
+            ip.out_off = out_off;
+            ip.in_off = b->epoch_in_off[e];
+            ip.in_channels = ep.channels;
+            const int inst = (int)b->insts.size();
+            for (int c = 0; c < C; ++c) b->blk_ic.push_back(make_int2(inst, c));
+            b->insts.push_back(ip);
+            ij_off += dp.nscales;
+            cen_off += C;
+            res_off += (long long)C * dp.N;
+            slot_off += dp.slots;
+            chunk_off += dp.chunks;
+            out_off += (long long)iters * C * 6;
+            b->cmax = std::max(b->cmax, C);
+        };
+        const bool smp = variant == EMPI_SMP || ep.channels == 1;  // src/empi.cpp:118
+        if (smp) {
+            for (int c = 0; c < ep.channels; ++c) add(1, c);
+        } else if (variant == EMPI_MMP2) {
+            add(1, -2);
+            for (int c = 0; c < ep.channels; ++c) b->fit_map.push_back(make_int2((int)b->insts.size() - 1, c));
+        } else {
+            add(ep.channels, -1);
+        }
+    }
+    b->nij = ij_off;
+    const int ninst = (int)b->insts.size();
+    const int band_cap = eng->opts.candidate_capacity > 0 ? eng->opts.candidate_capacity
+                                                          : std::max(8192, 64 * ninst);
+    CUDA_TRY(b->d_scales.alloc(b->scales.size()));
+    CUDA_TRY(b->d_dicts.alloc(b->dicts.size()));
+    CUDA_TRY(b->d_insts.alloc(ninst));
+    CUDA_TRY(b->d_blk_ic.alloc(b->blk_ic.size()));
+    CUDA_TRY(b->d_fit_map.alloc(b->fit_map.size()));
+    CUDA_TRY(b->d_input.alloc(b->total_in));
+    CUDA_TRY(b->d_residual.alloc(res_off));
+    CUDA_TRY(b->d_atoms.alloc(out_off));
+    CUDA_TRY(b->d_energies.alloc((size_t)ninst * iters));
+    CUDA_TRY(b->d_chan_energy.alloc(cen_off));
+    CUDA_TRY(b->d_fit_atoms.alloc(b->fit_map.size() * (size_t)iters * 6));
+    CUDA_TRY(b->d_stats.alloc(4));
+    CUDA_TRY(b->d_state.alloc(ninst));
+    CUDA_TRY(b->d_slots.alloc(slot_off));
+    CUDA_TRY(b->d_chunks.alloc(chunk_off));
+    CUDA_TRY(b->d_dirty.alloc(ij_off));
+    CUDA_TRY(b->d_crange.alloc(ij_off));
+    CUDA_TRY(b->d_ij_units.alloc(ij_off + ninst));
+    CUDA_TRY(b->d_ij_chunks.alloc(ij_off + ninst));
+    CUDA_TRY(b->d_inst_units.alloc(ninst + 1));
+    CUDA_TRY(b->d_inst_chunks.alloc(ninst + 1));
+    CUDA_TRY(b->d_ctr.alloc(CTR_COUNT));
+    CUDA_TRY(b->d_cslots.alloc(band_cap));
+    CUDA_TRY(b->d_cbins.alloc(band_cap));
+    CUDA_TRY(b->d_cbin_v.alloc((size_t)band_cap * b->cmax));
+    const int inst_bin_cap = 512;
+    CUDA_TRY(b->d_inst_bins.alloc((size_t)ninst * inst_bin_cap));
+    CUDA_TRY(b->d_indices.alloc((size_t)ninst * iters));
+    cudaStream_t s = eng->stream;
+    CUDA_TRY(cudaMemcpyAsync(b->d_scales.p, b->scales.data(), sizeof(ScalePlan) * b->scales.size(),
+                             cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(b->d_dicts.p, b->dicts.data(), sizeof(DictPlan) * b->dicts.size(),
+                             cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(b->d_insts.p, b->insts.data(), sizeof(InstPlan) * ninst, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(b->d_blk_ic.p, b->blk_ic.data(), sizeof(int2) * b->blk_ic.size(),
+                             cudaMemcpyHostToDevice, s));
+    if (!b->fit_map.empty())
+        CUDA_TRY(cudaMemcpyAsync(b->d_fit_map.p, b->fit_map.data(), sizeof(int2) * b->fit_map.size(),
+                                 cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemsetAsync(b->d_chunks.p, 0, sizeof(unsigned long long) * b->d_chunks.n, s));
+    CUDA_TRY(cudaMemsetAsync(b->d_slots.p, 0, sizeof(unsigned long long) * b->d_slots.n, s));
+    CUDA_TRY(cudaMemsetAsync(b->d_ctr.p, 0, sizeof(int) * CTR_COUNT, s));
+
+    BatchDev& d = b->dev;
+    d.scales = b->d_scales.p;
+    d.dicts = b->d_dicts.p;
+    d.insts = b->d_insts.p;
+    d.blk_ic = b->d_blk_ic.p;
+    d.tw = eng->tw;
+    d.input = b->d_input.p;
+    d.ninst = ninst;
+    d.nblk_ic = (int)b->blk_ic.size();
+    d.cmax = b->cmax;
+    d.iter_max = iters;
+    d.mode = b->mode;
+    d.residual_energy = b->settings.residual_energy;
+    d.band = (float)eng->opts.candidate_band;
+    d.cslot_cap = band_cap;
+    d.cbin_cap = band_cap;
+    d.inst_bin_cap = inst_bin_cap;
+    d.residual = b->d_residual.p;
+    d.state = b->d_state.p;
+    d.slots = b->d_slots.p;
+    d.chunks = b->d_chunks.p;
+    d.dirty = b->d_dirty.p;
+    d.ij_units = b->d_ij_units.p;
+    d.ij_chunks = b->d_ij_chunks.p;
+    d.ij_crange = b->d_crange.p;
+    d.inst_units = b->d_inst_units.p;
+    d.inst_chunks = b->d_inst_chunks.p;
+    d.ctr = b->d_ctr.p;
+    d.cslots = b->d_cslots.p;
+    d.cbins = b->d_cbins.p;
+    d.cbin_v = b->d_cbin_v.p;
+    d.inst_bins = b->d_inst_bins.p;
+    d.atoms = b->d_atoms.p;
+    d.energies = b->d_energies.p;
+    d.indices = b->d_indices.p;
+    d.chan_energy = b->d_chan_energy.p;
+    d.stats = b->d_stats.p;
+    d.dump = nullptr;
+    st = configure(b.get());
+    if (st != EMPI_OK) return st;
+    b->tree_grid = eng->sms * 8;
+    b->rescore_grid = eng->sms * 4;
+    if (b->max_n * sizeof(double) > 48 * 1024 && !b->fit_map.empty()) {
+        CUDA_TRY(cudaFuncSetAttribute(k_mmp2_fit, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(b->max_n * sizeof(double))));
+    }
+    if (b->max_n * sizeof(double) > 200 * 1024 && !b->fit_map.empty())
+        return fail(EMPI_ERR_INVALID_ARGUMENT, "epochTooLongForMmp2Fit");
+    CUDA_TRY(cudaEventCreate(&b->run_start));
+    CUDA_TRY(cudaEventCreate(&b->run_stop));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    *out = b.release();
+    return ok();
+}
+
+empi_status check_errors(empi_batch* b) {
+    std::vector<InstState> st(b->insts.size());
+    CUDA_TRY(cudaMemcpyAsync(st.data(), b->d_state.p, sizeof(InstState) * st.size(), cudaMemcpyDeviceToHost,
+                             b->eng->stream));
+    CUDA_TRY(cudaStreamSynchronize(b->eng->stream));
+    for (size_t i = 0; i < st.size(); ++i) {
+        if (st[i].status == ST_ERROR || st[i].err != ERR_NONE) {
+            switch (st[i].err) {
+                case ERR_SIGNAL_EMPTY: return fail(EMPI_ERR_SIGNAL_IS_EMPTY, "signalIsEmpty");
+                case ERR_MAP_EMPTY: return fail(EMPI_ERR_ENERGY_MAP_IS_EMPTY, "energyMapIsEmpty");
+                case ERR_CAND_OVERFLOW: return fail(EMPI_ERR_CANDIDATE_OVERFLOW, "candidateOverflow");
+                default: return fail(EMPI_ERR_INTERNAL, "internalError");
+            }
+        }
+    }
+    return EMPI_OK;
+}
+
+empi_status capture_graph(empi_batch* b) {
+    if (b->graph) return EMPI_OK;
+    const int K = b->eng->opts.iterations_per_graph;
+    cudaStream_t s = b->eng->stream;
+    const bool timing = b->eng->opts.timing != 0;
+    if (timing && b->ev.empty()) {
+        b->ev.resize(2 * (K + 1));
+        for (auto& e : b->ev) CUDA_TRY(cudaEventCreate(&e));
+    }
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < K; ++k)
+        launch_iteration(b, s, timing ? b->ev[2 * (k + 1)] : nullptr, timing ? b->ev[2 * (k + 1) + 1] : nullptr);
+    cudaError_t ce = cudaStreamEndCapture(s, &g);
+    if (ce != cudaSuccess) return fail(EMPI_ERR_CUDA, std::string("cuda: ") + cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) return fail(EMPI_ERR_CUDA, std::string("cuda: ") + cudaGetErrorString(ce));
+    b->graph_iters = K;
+    return EMPI_OK;
+}
+
+}  // namespace
+
+extern "C" empi_status empi_batch_create(empi_engine* eng, empi_variant variant, const empi_dictionary* dict,
+                                         const empi_settings* settings, const empi_epoch* epochs, int count,
+                                         empi_batch** out) {
+    if (!settings) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    return build_batch(eng, (int)variant, dict, settings, epochs, count, settings->iteration_max, out);
+}
+
+extern "C" void empi_batch_destroy(empi_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->eng->device);
+    cudaStreamSynchronize(b->eng->stream);
+    delete b;
+}
+
+extern "C" empi_status empi_batch_load(empi_batch* b, const empi_epoch* epochs) {
+    if (!b || !epochs) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    empi_status st = set_device(b->eng);
+    if (st != EMPI_OK) return st;
+    for (size_t e = 0; e < b->epochs.size(); ++e) {
+        if (epochs[e].channels != b->epochs[e].channels || epochs[e].samples != b->epochs[e].samples || !epochs[e].data)
+            return fail(EMPI_ERR_INVALID_ARGUMENT, "epochShapeMismatch");
+        CUDA_TRY(cudaMemcpyAsync(b->d_input.p + b->epoch_in_off[e], epochs[e].data,
+                                 sizeof(float) * (size_t)epochs[e].channels * epochs[e].samples,
+                                 cudaMemcpyHostToDevice, b->eng->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(b->eng->stream));
+    return ok();
+}
+
+namespace empi {
+
+empi_status batch_load_device(empi_batch* b, const float* const* device_data) {
+    for (size_t e = 0; e < b->epochs.size(); ++e)
+        CUDA_TRY(cudaMemcpyAsync(b->d_input.p + b->epoch_in_off[e], device_data[e],
+                                 sizeof(float) * (size_t)b->epochs[e].channels * b->epochs[e].samples,
+                                 cudaMemcpyDeviceToDevice, b->eng->stream));
+    return EMPI_OK;
+}
+
+}  // namespace empi
+
+extern "C" empi_status empi_batch_run(empi_batch* b) {
+    if (!b) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    empi_status st = set_device(b->eng);
+    if (st != EMPI_OK) return st;
+    st = capture_graph(b);
+    if (st != EMPI_OK) return st;
+    cudaStream_t s = b->eng->stream;
+    const bool timing = b->eng->opts.timing != 0;
+    CUDA_TRY(cudaMemsetAsync(b->d_ctr.p, 0, sizeof(int) * CTR_COUNT, s));
+    CUDA_TRY(cudaMemsetAsync(b->d_stats.p, 0, sizeof(double) * 4, s));
+    CUDA_TRY(cudaMemsetAsync(b->d_energies.p, 0xff, sizeof(double) * b->d_energies.n, s));  // NaN
+    CUDA_TRY(cudaEventRecord(b->run_start, s));
+    k_init<<<(int)b->blk_ic.size(), 256, 0, s>>>(b->dev, 1);
+    launch_update(b, SCHED_INIT, -1, 0.0, 0.0, s, timing ? b->ev[0] : nullptr, timing ? b->ev[1] : nullptr);
+    int launches = 7;
+    double refresh_ms = 0.0;
+    int refresh_launches = 0;
+    if (timing) {
+        CUDA_TRY(cudaStreamSynchronize(s));
+        float ms = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]));
+        refresh_ms += ms;
+        refresh_launches++;
+    }
+    int iters = 0;
+    const int imax = b->settings.iteration_max;
+    int active = 1;
+    while (iters < imax && active > 0) {
+        CUDA_TRY(cudaGraphLaunch(b->graph, s));
+        iters += b->graph_iters;
+        launches += b->graph_iters * b->launches_per_iter;
+        CUDA_TRY(cudaMemcpyAsync(&active, b->d_ctr.p + CTR_ACTIVE, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        if (timing) {
+            for (int k = 0; k < b->graph_iters; ++k) {
+                float ms = 0.f;
+                CUDA_TRY(cudaEventElapsedTime(&ms, b->ev[2 * (k + 1)], b->ev[2 * (k + 1) + 1]));
+                refresh_ms += ms;
+                refresh_launches++;
+            }
+        }
+    }
+    if (!b->fit_map.empty()) {
+        k_mmp2_fit<<<(int)b->fit_map.size(), 256, b->max_n * sizeof(double), s>>>(b->dev, b->d_fit_map.p,
+                                                                                 b->d_fit_atoms.p, imax);
+        launches++;
+    }
+    CUDA_TRY(cudaEventRecord(b->run_stop, s));
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(s));
+    float run_ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&run_ms, b->run_start, b->run_stop));
+    int ctr[CTR_COUNT];
+    double stats[4];
+    CUDA_TRY(cudaMemcpy(ctr, b->d_ctr.p, sizeof(ctr), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(stats, b->d_stats.p, sizeof(stats), cudaMemcpyDeviceToHost));
+    std::vector<InstState> sts(b->insts.size());
+    CUDA_TRY(cudaMemcpy(sts.data(), b->d_state.p, sizeof(InstState) * sts.size(), cudaMemcpyDeviceToHost));
+    b->stats = empi_batch_stats{};
+    int maxit = 0, natoms = 0;
+    for (auto& x : sts) {
+        maxit = std::max(maxit, x.it);
+        natoms += x.it;
+    }
+    b->stats.iterations = maxit;
+    b->stats.atoms = natoms;
+    b->stats.refresh_units = ctr[CTR_STAT_UNITS];
+    b->stats.windows = (long long)stats[2];
+    b->stats.fft_flops = stats[0];
+    b->stats.refresh_ms = refresh_ms;
+    b->stats.refresh_launches = refresh_launches;
+    b->stats.kernel_launches = launches;
+    b->stats.candidate_bins = ctr[CTR_STAT_BINS];
+    b->stats.run_ms = run_ms;
+    b->stats.algorithmic_bytes = stats[1];
+    empi_status es = check_errors(b);
+    if (es != EMPI_OK) return es;
+    return ok();
+}
+
+extern "C" empi_status empi_batch_atoms(empi_batch* b, int epoch, int cap, double* atoms, int* count,
+                                        double* energies, int* indices) {
+    if (!b || epoch < 0 || epoch >= (int)b->epochs.size() || cap < 0 || (cap > 0 && !atoms))
+        return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    empi_status st = set_device(b->eng);
+    if (st != EMPI_OK) return st;
+    const int C = b->epochs[epoch].channels;
+    const int iters = b->settings.iteration_max;
+    const int i0 = b->epoch_first_inst[epoch];
+    const InstPlan& ip0 = b->insts[i0];
+    const int ninst_e = (ip0.chan0 >= 0) ? C : 1;  // SMP: one loop per channel
+    std::vector<InstState> sts(ninst_e);
+    CUDA_TRY(cudaMemcpy(sts.data(), b->d_state.p + i0, sizeof(InstState) * ninst_e, cudaMemcpyDeviceToHost));
+    std::vector<double> en((size_t)ninst_e * iters);
+    std::vector<int4> ind((size_t)ninst_e * iters);
+    CUDA_TRY(cudaMemcpy(en.data(), b->d_energies.p + (size_t)i0 * iters, sizeof(double) * en.size(),
+                        cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(ind.data(), b->d_indices.p + (size_t)i0 * iters, sizeof(int4) * ind.size(),
+                        cudaMemcpyDeviceToHost));
+    const int lim = std::min(cap, iters);
+    if (ip0.chan0 >= 0) {  // SMP
+        for (int c = 0; c < C; ++c) {
+            const InstPlan& ip = b->insts[i0 + c];
+            const int n = std::min(sts[c].it, lim);
+            if (count) count[c] = sts[c].it;
+            if (n > 0)
+                CUDA_TRY(cudaMemcpy(atoms + (size_t)c * cap * 6, b->d_atoms.p + ip.out_off, sizeof(double) * 6 * n,
+                                    cudaMemcpyDeviceToHost));
+            for (int a = 0; a < lim; ++a) {
+                if (energies) energies[(size_t)c * cap + a] = en[(size_t)c * iters + a];
+                if (indices) {
+                    const int4 v = ind[(size_t)c * iters + a];
+                    indices[((size_t)c * cap + a) * 3] = v.x;
+                    indices[((size_t)c * cap + a) * 3 + 1] = v.y;
+                    indices[((size_t)c * cap + a) * 3 + 2] = v.z;
+                }
+            }
+        }
+    } else {
+        const int n = std::min(sts[0].it, lim);
+        if (count)
+            for (int c = 0; c < C; ++c) count[c] = sts[0].it;
+        if (ip0.chan0 == -2) {  // MMP2: per-channel fits
+            const int f0 = b->epoch_first_fit[epoch];
+            for (int c = 0; c < C; ++c)
+                if (n > 0)
+                    CUDA_TRY(cudaMemcpy(atoms + (size_t)c * cap * 6, b->d_fit_atoms.p + ((size_t)(f0 + c) * iters) * 6,
+                                        sizeof(double) * 6 * n, cudaMemcpyDeviceToHost));
+        } else {
+            std::vector<double> tmp((size_t)std::max(n, 1) * C * 6);
+            if (n > 0)
+                CUDA_TRY(cudaMemcpy(tmp.data(), b->d_atoms.p + ip0.out_off, sizeof(double) * tmp.size(),
+                                    cudaMemcpyDeviceToHost));
+            for (int a = 0; a < n; ++a)
+                for (int c = 0; c < C; ++c)
+                    std::memcpy(atoms + ((size_t)c * cap + a) * 6, tmp.data() + ((size_t)a * C + c) * 6,
+                                sizeof(double) * 6);
+        }
+        for (int a = 0; a < lim; ++a) {
+            if (energies) energies[a] = en[a];
+            if (indices) {
+                indices[a * 3] = ind[a].x;
+                indices[a * 3 + 1] = ind[a].y;
+                indices[a * 3 + 2] = ind[a].z;
+            }
+        }
+    }
+    return ok();
+}
+
+extern "C" empi_status empi_batch_total_energy(empi_batch* b, int epoch, double* totals) {
+    if (!b || !totals || epoch < 0 || epoch >= (int)b->epochs.size())
+        return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    empi_status st = set_device(b->eng);
+    if (st != EMPI_OK) return st;
+    const int i0 = b->epoch_first_inst[epoch];
+    const int n = b->insts[i0].chan0 >= 0 ? b->epochs[epoch].channels : 1;
+    std::vector<InstState> sts(n);
+    CUDA_TRY(cudaMemcpy(sts.data(), b->d_state.p + i0, sizeof(InstState) * n, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) totals[i] = sts[i].etotal;
+    return ok();
+}
+
+extern "C" empi_status empi_batch_get_stats(empi_batch* b, empi_batch_stats* out) {
+    if (!b || !out) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    *out = b->stats;
+    return ok();
+}
+
+extern "C" empi_status empi_decompose(empi_engine* eng, empi_variant variant, const empi_dictionary* dict,
+                                      const empi_settings* settings, const empi_epoch* epochs, int count, int cap,
+                                      double* atoms, int* counts) {
+    empi_batch* b = nullptr;
+    empi_status st = empi_batch_create(eng, variant, dict, settings, epochs, count, &b);
+    if (st != EMPI_OK) return st;
+    std::unique_ptr<empi_batch, void (*)(empi_batch*)> guard(b, empi_batch_destroy);
+    st = empi_batch_load(b, epochs);
+    if (st != EMPI_OK) return st;
+    st = empi_batch_run(b);
+    if (st != EMPI_OK) return st;
+    size_t off = 0, coff = 0;
+    for (int e = 0; e < count; ++e) {
+        st = empi_batch_atoms(b, e, cap, atoms ? atoms + off : nullptr, counts ? counts + coff : nullptr, nullptr,
+                              nullptr);
+        if (st != EMPI_OK) return st;
+        off += (size_t)epochs[e].channels * cap * 6;
+        coff += epochs[e].channels;
+    }
+    return ok();
+}
+
+// ------------------------------------------------------------ workspace seam
+
+struct empi_workspace {
+    empi_batch* b = nullptr;
+    int C = 0, N = 0;
+    double fs = 0;
+    double* d_params = nullptr;
+    ~empi_workspace() {
+        if (d_params) cudaFree(d_params);
+        if (b) empi_batch_destroy(b);
+    }
+};
+
+namespace {
+
+empi_status ws_reset_state(empi_workspace* w) {
+    empi_batch* b = w->b;
+    cudaStream_t s = b->eng->stream;
+    CUDA_TRY(cudaMemset2DAsync(b->d_state.p, sizeof(InstState), 0, 4 * sizeof(int), b->insts.size(), s));
+    CUDA_TRY(cudaMemsetAsync(b->d_ctr.p + CTR_CSLOTS, 0, sizeof(int) * 4, s));
+    return EMPI_OK;
+}
+
+}  // namespace
+
+extern "C" empi_status empi_workspace_create(empi_engine* eng, const empi_dictionary* dict, double fs, int channels,
+                                             int samples, empi_variant variant, empi_workspace** out) {
+    if (!eng || !dict || !out || channels <= 0) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    *out = nullptr;
+    std::unique_ptr<empi_workspace> w(new empi_workspace);
+    empi_epoch ep{fs, channels, samples, nullptr};
+    empi_settings set{1, 0.0};
+    const int v = channels == 1 ? EMPI_SMP : (variant == EMPI_MMP1 ? EMPI_MMP1 : EMPI_MMP3);
+    empi_status st = build_batch(eng, v, dict, &set, &ep, 1, 1, &w->b);
+    if (st != EMPI_OK) return st;
+    w->C = channels;
+    w->N = samples;
+    w->fs = fs;
+    CUDA_TRY(cudaMalloc(&w->d_params, sizeof(double) * 6 * channels));
+    *out = w.release();
+    return ok();
+}
+
+extern "C" void empi_workspace_destroy(empi_workspace* w) { delete w; }
+
+extern "C" empi_status empi_workspace_compute(empi_workspace* w, const double* samples) {
+    if (!w || !samples) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    empi_batch* b = w->b;
+    empi_status st = set_device(b->eng);
+    if (st != EMPI_OK) return st;
+    cudaStream_t s = b->eng->stream;
+    CUDA_TRY(cudaMemcpyAsync(b->d_residual.p, samples, sizeof(double) * (size_t)w->C * w->N, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemsetAsync(b->d_ctr.p, 0, sizeof(int) * CTR_COUNT, s));
+    k_init<<<(int)b->blk_ic.size(), 256, 0, s>>>(b->dev, 0);
+    launch_update(b, SCHED_INIT, -1, 0.0, 0.0, s, nullptr, nullptr);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return ok();
+}
+
+extern "C" empi_status empi_workspace_find_best(empi_workspace* w, double* params, int* index) {
+    if (!w || !params) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    empi_batch* b = w->b;
+    empi_status st = set_device(b->eng);
+    if (st != EMPI_OK) return st;
+    cudaStream_t s = b->eng->stream;
+    st = ws_reset_state(w);
+    if (st != EMPI_OK) return st;
+    launch_select(b, s);
+    CUDA_TRY(cudaGetLastError());
+    st = check_errors(b);
+    if (st != EMPI_OK) return st;
+    CUDA_TRY(cudaMemcpy(params, b->d_atoms.p, sizeof(double) * 6 * w->C, cudaMemcpyDeviceToHost));
+    if (index) {
+        int4 v;
+        CUDA_TRY(cudaMemcpy(&v, b->d_indices.p, sizeof(int4), cudaMemcpyDeviceToHost));
+        index[0] = v.x;
+        index[1] = v.y;
+        index[2] = v.z;
+    }
+    return ok();
+}
+
+extern "C" empi_status empi_workspace_atom_count(const empi_workspace* w, uint64_t* count) {
+    if (!w || !count) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    *count = w->b->dicts[0].values;
+    return ok();
+}
+
+extern "C" empi_status empi_workspace_subtract_atom(empi_workspace* w, const double* params, double* samples,
+                                                    int channel) {
+    if (!w || !params || !samples || channel < 0 || channel >= w->C)
+        return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    empi_batch* b = w->b;
+    empi_status st = set_device(b->eng);
+    if (st != EMPI_OK) return st;
+    cudaStream_t s = b->eng->stream;
+    double* x = b->d_residual.p + (size_t)channel * w->N;
+    CUDA_TRY(cudaMemcpyAsync(x, samples, sizeof(double) * w->N, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(w->d_params, params, sizeof(double) * 6, cudaMemcpyHostToDevice, s));
+    k_subtract_signal<<<1, 256, 0, s>>>(x, w->N, w->fs, w->d_params, 0);
+    CUDA_TRY(cudaMemcpyAsync(samples, x, sizeof(double) * w->N, cudaMemcpyDeviceToHost, s));
+    st = ws_reset_state(w);
+    if (st != EMPI_OK) return st;
+    // src/gabor.cpp:189-209: refresh every window within 3 (s + sA) of tA
+    launch_update(b, SCHED_ATOM, -1, params[2] / w->fs, params[3] / w->fs, s, nullptr, nullptr);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return ok();
+}
+
+extern "C" empi_status empi_workspace_energy_map(empi_workspace* w, int scale, float* energy) {
+    if (!w || !energy) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    empi_batch* b = w->b;
+    if (scale < 0 || scale >= b->dicts[0].nscales) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidScale");
+    empi_status st = set_device(b->eng);
+    if (st != EMPI_OK) return st;
+    const ScalePlan& sp = b->scales[scale];
+    const size_t n = (size_t)sp.fcount * sp.tcount;
+    DevBuf<float> dump;
+    CUDA_TRY(dump.alloc(n));
+    cudaStream_t s = b->eng->stream;
+    CUDA_TRY(cudaMemsetAsync(dump.p, 0, sizeof(float) * n, s));
+    st = ws_reset_state(w);
+    if (st != EMPI_OK) return st;
+    b->dev.dump = dump.p;
+    launch_update(b, SCHED_INIT, scale, 0.0, 0.0, s, nullptr, nullptr);
+    b->dev.dump = nullptr;
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(energy, dump.p, sizeof(float) * n, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return ok();
+}
+
+extern "C" empi_status empi_subtract_atom_from_signal(empi_engine* eng, double* params, double* samples, int n,
+                                                      double fs, int fit) {
+    if (!eng || !params || !samples || n <= 0 || !(fs > 0)) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    empi_status st = set_device(eng);
+    if (st != EMPI_OK) return st;
+    DevBuf<double> x, p;
+    CUDA_TRY(x.alloc(n));
+    CUDA_TRY(p.alloc(6));
+    cudaStream_t s = eng->stream;
+    CUDA_TRY(cudaMemcpyAsync(x.p, samples, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(p.p, params, sizeof(double) * 6, cudaMemcpyHostToDevice, s));
+    k_subtract_signal<<<1, 256, 0, s>>>(x.p, n, fs, p.p, fit);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(samples, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(params, p.p, sizeof(double) * 6, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return ok();
+}

@@ -1,0 +1,169 @@
+// Host-side dictionary geometry and per-scale transform plans.
+#include "geometry.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+
+namespace empi {
+
+namespace {
+
+const double kGaussHalfWidth = 3.0;     // src/gabor.cpp:14
+const double kMinScaleInSamples = 2.0;  // src/gabor.cpp:19
+
+long pow2_round(long x) {  // inc/fftw.hpp:161-168
+    long y = 2;
+    while (y < x) y *= 2;
+    return y;
+}
+
+int ilog2(long x) {
+    int l = 0;
+    while ((1L << l) < x) ++l;
+    return l;
+}
+
+}  // namespace
+
+bool build_dictionary(double fs, int N, double energyError, double scaleMin, double scaleMax,
+                      double freqMax, int lcap, DictPlan& dict, std::vector<ScalePlan>& scales,
+                      std::string& err) {
+    if (!(fs > 0.0) || !std::isfinite(fs)) {
+        err = "invalidSamplingFrequency";
+        return false;
+    }
+    if (!(energyError > 0.0 && energyError < 1.0)) {
+        err = "invalidEnergyErrorValue";
+        return false;
+    }
+    if (N < 4) {
+        err = "signalIsTooShortForThisDecomposition";
+        return false;
+    }
+    if (lcap < 16 || lcap > kUnitPoints / 2 || (lcap & (lcap - 1))) {
+        err = "invalidTransformCap";
+        return false;
+    }
+    // GaborWorkspaceBuilder::prepareWorkspace, src/gabor.cpp:213-252
+    const double smin = std::max(scaleMin, kMinScaleInSamples / fs);
+    const double smax = std::min(scaleMax, N / fs);
+    const double root = std::sqrt(-2.0 / M_PI * std::log(1.0 - energyError));
+    const double aDenomSqrt = 1.0 - energyError;
+    const double aNominPart =
+        energyError * (2.0 - energyError) * (energyError * energyError - 2 * energyError + 2);
+    const double a = (1.0 + std::sqrt(aNominPart)) / (aDenomSqrt * aDenomSqrt);
+    const double dl = std::log(a);
+    const double tMax = (N - 1) / fs;
+    const double lMin = std::log(smin);
+    const double lMax = std::log(smax);
+    const long lCount = std::lrint((lMax - lMin) / dl + 0.5) + 1;
+    if (lCount < 2 || !(smax >= smin)) {
+        err = "invalidDictionary";
+        return false;
+    }
+    dict = DictPlan{};
+    dict.fs = fs;
+    dict.tMax = tMax;
+    dict.N = N;
+    dict.scale0 = (int)scales.size();
+    dict.nscales = (int)lCount;
+    long long slots = 0;
+    unsigned long long values = 0;
+    for (long i = 0; i < lCount; ++i) {
+        ScalePlan p{};
+        const double s = std::exp(lMin + i * (lMax - lMin) / (lCount - 1));
+        const double dt = root * s;
+        const double df = root / s;
+        const double hw = kGaussHalfWidth * s;
+        const long Ngauss = 2 * std::lrint(hw * fs - 0.5) + 1;
+        const long Nfft = pow2_round(std::max(Ngauss, std::lrint(fs / df + 0.5)));
+        const long tCount = std::lrint(tMax / dt + 0.5) + 1;
+        if (std::max(Nfft, tCount) > static_cast<long>(std::numeric_limits<int>::max())) {
+            err = "signalFileIsTooLongForThisDecomposition";
+            return false;
+        }
+        long fCount = Nfft / 2 + 1;
+        if (std::isfinite(freqMax) && freqMax > 0) {
+            fCount = std::min(fCount, std::lrint(freqMax / fs * Nfft + 0.5) + 1);
+        }
+        if (!std::isfinite(s) || tCount < 2 || fCount < 1) {
+            err = "invalidDictionary";
+            return false;
+        }
+        p.s = s;
+        p.hw = hw;
+        p.nfft = (int)Nfft;
+        p.fcount = (int)fCount;
+        p.tcount = (int)tCount;
+
+        // longest window over the time grid (src/gabor.cpp:279-292)
+        int wmax = 1;
+        for (long ti = 0; ti < tCount; ++ti) {
+            const double t0 = ti * tMax / (tCount - 1);
+            long l = std::lrint((t0 - hw) * fs), r = std::lrint((t0 + hw) * fs);
+            long iL = std::max(0L, l), iR = std::min((long)N - 1, r);
+            wmax = std::max(wmax, (int)(iR - iL + 1));
+        }
+        if (wmax > Nfft) {
+            // the reference would write past its FFT buffer here
+            err = "windowLongerThanTransform";
+            return false;
+        }
+        p.wmax = wmax;
+
+        const long Nh = Nfft / 2;
+        const long zlen = (wmax + 1) / 2;
+        long L = std::min(Nh, pow2_round(std::max(zlen, 1L)));
+        if (Nh == 1) L = 1;
+        L = std::min(L, (long)lcap);
+        p.L = (int)L;
+        p.logL = ilog2(L);
+        p.M = (int)(Nh / L);
+        p.F = (int)((zlen + L - 1) / L);
+        if (p.F < 1) p.F = 1;
+        p.G = p.M == 1 ? 1 : (p.M == 2 ? 2 : p.M / 2 + 1);
+        p.B1 = std::min(kMaxWindowsPerUnit, (int)(kUnitPoints / L));
+        p.B2 = std::max(1, std::min(kMaxWindowsPerUnit, (int)(kUnitPoints / (2 * L))));
+
+        // bins whose normalisation depends on the phase (expFactor >= 2^-30),
+        // and the first "high frequency" bin (src/gabor.cpp:44-52)
+        const double thr = std::ldexp(1.0, -30);
+        const double nyq = 0.5 * fs;
+        int khf = (int)fCount;
+        for (long k = 0; k < fCount; ++k) {
+            double f = k * fs / Nfft;
+            if (f > 0.5 * nyq) {
+                khf = (int)k;
+                break;
+            }
+        }
+        auto need = [&](long k) {
+            double f = k * fs / Nfft;
+            bool high = f > 0.5 * nyq;
+            double f4 = high ? (nyq - f) : f;
+            double e = std::exp(-2 * M_PI * s * s * f4 * f4);
+            return e >= thr;
+        };
+        int klo = 0;
+        while (klo < khf && need(klo)) ++klo;
+        int khi = (int)fCount - 1;
+        while (khi >= khf && need(khi)) --khi;
+        p.klo = klo;
+        p.khi = khi;
+        p.khf = khf;
+        p.slot_base = slots;
+        p.aG = (float)(std::sqrt(M_PI) / (s * fs));
+        p.Kc = (float)(2.0 * M_SQRT2 / (s * fs));
+        p.K1 = (float)(M_SQRT2 / (s * fs));
+        slots += (long long)tCount * p.G;
+        values += (unsigned long long)fCount * (unsigned long long)tCount;
+        scales.push_back(p);
+    }
+    dict.slots = slots;
+    dict.chunks = (int)((slots + kChunk - 1) / kChunk);
+    dict.values = values;
+    return true;
+}
+
+}  // namespace empi

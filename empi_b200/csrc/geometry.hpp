@@ -1,0 +1,17 @@
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "plan.hpp"
+
+namespace empi {
+
+// Appends the scales of one dictionary (fs, N, energyError, scale/frequency
+// limits) to `scales` and fills `dict`.  Returns false with a camelCase
+// message in `err` on invalid input.
+bool build_dictionary(double fs, int N, double energyError, double scaleMin, double scaleMax,
+                      double freqMax, int lcap, DictPlan& dict, std::vector<ScalePlan>& scales,
+                      std::string& err);
+
+}  // namespace empi

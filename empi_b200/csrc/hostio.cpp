@@ -1,0 +1,404 @@
+// Host surface kept from empi: the key/value config file, the float32 signal
+// reader, the SVAROG (MPv5) book writer and the CLI driver with its stdout
+// progress protocol.  Decomposition itself is one batched device run over all
+// epochs read from the file.
+#include <algorithm>
+#include <cctype>
+#include <climits>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/empi_b200.h"
+#include "engine.hpp"
+
+namespace {
+
+struct Error : std::runtime_error {
+    empi_status status;
+    Error(empi_status st, const std::string& m) : std::runtime_error(m), status(st) {}
+};
+
+// ------------------------------------------------------------ configuration
+
+// Configuration::parse/has/at, src/conf.cpp:10-48: "name<ws>value" lines,
+// '#' starts a comment line, the value runs to the end of the line.
+class Configuration {
+    std::map<std::string, std::string> values;
+
+public:
+    void parse(const std::string& path) {
+        std::ifstream stream(path);
+        if (!stream) throw Error(EMPI_ERR_CONFIG, "couldNotOpenConfigFile");
+        values.clear();
+        std::string line;
+        while (std::getline(stream, line)) {
+            std::string::size_type iname = line.find_first_not_of(" \t");
+            if (iname == std::string::npos || line[iname] == '#') continue;
+            std::string::size_type ispace = line.find_first_of(" \t", iname + 1);
+            if (ispace == std::string::npos) continue;
+            std::string::size_type ivalue = line.find_first_not_of(" \t", ispace + 1);
+            if (ivalue == std::string::npos) continue;
+            std::string name = line.substr(iname, ispace - iname);
+            std::string value = line.substr(ivalue);
+            if (!name.empty() && !value.empty()) values[name] = value;
+        }
+    }
+    bool has(const std::string& key) const { return values.count(key) != 0; }
+    const std::string& at(const std::string& key) const {
+        auto it = values.find(key);
+        if (it == values.end()) throw Error(EMPI_ERR_CONFIG, "missingConfigurationEntry:" + key);
+        return it->second;
+    }
+};
+
+// parseIntegerSubset, src/empi.cpp:22-47 ("1-3,5")
+std::vector<int> parse_subset(const std::string& text, int max) {
+    std::stringstream ss(text);
+    std::string item;
+    std::vector<int> numbers;
+    while (std::getline(ss, item, ',')) {
+        int start, end;
+        int status = sscanf(item.c_str(), "%d-%d", &start, &end);
+        if (status == 2 && start >= 1 && end <= max) {
+            for (int i = start; i <= end; ++i) numbers.push_back(i);
+        } else if (status == 1 && start >= 1 && start <= max) {
+            numbers.push_back(start);
+        } else {
+            throw Error(EMPI_ERR_CONFIG, "invalidSubsetSpecification");
+        }
+    }
+    if (numbers.empty()) throw Error(EMPI_ERR_CONFIG, "emptySubsetSpecification");
+    return numbers;
+}
+
+// ------------------------------------------------------------ signal reader
+
+// SignalReader and its three modes, src/io.cpp:9-85.  Samples are float32,
+// channels interleaved; the selected channels are kept (1-based).
+class SignalReader {
+    FILE* file = nullptr;
+    int mode = 0;  // 0 all epochs, 1 selected epochs, 2 whole signal
+    int epochSize = 0;
+    std::vector<int> epochs;
+    size_t nextEpoch = 0;
+    bool wholeDone = false;
+
+public:
+    std::string path;
+    int channelCount = 0;
+    double freqSampling = 0;
+    std::vector<int> selectedChannels;
+
+    SignalReader(const std::string& p, int mode_, int epochSize_, std::vector<int> epochs_)
+        : mode(mode_), epochSize(epochSize_), epochs(std::move(epochs_)), path(p) {
+        file = fopen(p.c_str(), "rb");
+        if (!file) throw Error(EMPI_ERR_IO, "couldNotOpenSignalFile");
+    }
+    ~SignalReader() {
+        if (file) fclose(file);
+    }
+
+    // returns samples x C (selected channels), interleaved; empty at the end
+    std::vector<float> readEpoch(long samplesToRead, int& count) {
+        const int C = (int)selectedChannels.size();
+        std::vector<float> out;
+        std::vector<float> frame(channelCount);
+        long left = INT_MAX;
+        count = 0;
+        while (samplesToRead-- > 0 &&
+               fread(frame.data(), sizeof(float), channelCount, file) == (size_t)channelCount) {
+            if (--left < 0) throw Error(EMPI_ERR_IO, "signalFileIsTooLongForThisMachine");
+            for (int i = 0; i < C; ++i) out.push_back(frame[selectedChannels[i] - 1]);
+            ++count;
+        }
+        return out;
+    }
+
+    std::vector<float> read(int& count) {
+        if (mode == 0) {
+            std::vector<float> r = readEpoch(epochSize, count);
+            if (count > 0 && count != epochSize) throw Error(EMPI_ERR_IO, "fileIsTruncated");
+            return r;
+        }
+        if (mode == 1) {
+            if (nextEpoch >= epochs.size()) {
+                count = 0;
+                return {};
+            }
+            int epoch = epochs[nextEpoch++];
+            if (fseek(file, (long)sizeof(float) * channelCount * (long)epochSize * (epoch - 1), SEEK_SET))
+                throw Error(EMPI_ERR_IO, "signalSeekFailed");
+            std::vector<float> r = readEpoch(epochSize, count);
+            if (count != epochSize) throw Error(EMPI_ERR_IO, "fileIsTruncated");
+            return r;
+        }
+        if (wholeDone) {
+            count = 0;
+            return {};
+        }
+        wholeDone = true;
+        return readEpoch(INT_MAX, count);
+    }
+};
+
+// ------------------------------------------------------------ book writer
+
+// Big-endian encoders (inc/io.hpp:18-61)
+void put_u8(std::vector<uint8_t>& b, unsigned v) { b.push_back((uint8_t)v); }
+void put_u16(std::vector<uint8_t>& b, unsigned v) {
+    b.push_back((uint8_t)(v >> 8));
+    b.push_back((uint8_t)v);
+}
+void put_u32(std::vector<uint8_t>& b, uint32_t v) {
+    b.push_back((uint8_t)(v >> 24));
+    b.push_back((uint8_t)(v >> 16));
+    b.push_back((uint8_t)(v >> 8));
+    b.push_back((uint8_t)v);
+}
+void put_f32(std::vector<uint8_t>& b, double v) {
+    float f = (float)v;
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    put_u32(b, u);
+}
+void set_u32(std::vector<uint8_t>& b, size_t at, uint32_t v) {
+    b[at] = (uint8_t)(v >> 24);
+    b[at + 1] = (uint8_t)(v >> 16);
+    b[at + 2] = (uint8_t)(v >> 8);
+    b[at + 3] = (uint8_t)v;
+}
+
+// MPv5 header: version, comment "empi", signal and decomposition info with the
+// constant fields of src/io.cpp:111-117 (inc/io.hpp:65-98 layout).
+void book_header(std::vector<uint8_t>& b, int C, double fs) {
+    const char version[6] = {'M', 'P', 'v', '5', '.', '0'};
+    b.insert(b.end(), version, version + 6);
+    put_u8(b, 1);
+    put_u32(b, 4);
+    const char comment[4] = {'e', 'm', 'p', 'i'};
+    b.insert(b.end(), comment, comment + 4);
+    put_u8(b, 2);
+    put_u32(b, 27);
+    put_u8(b, 5);
+    put_u8(b, 10);
+    put_f32(b, fs);
+    put_f32(b, 1.0);   // pointsPerMicrovolt
+    put_u16(b, (unsigned)C);
+    put_u8(b, 6);
+    put_u8(b, 13);
+    put_f32(b, 100.0); // energyPercent
+    put_u32(b, 1);     // iterationCount
+    put_u32(b, 0);     // dictionarySize
+    put_u8(b, 'F');
+}
+
+// One epoch block (BookWriter::write, src/io.cpp:119-167): signal and atoms
+// per channel, with lengths patched after the fact.
+void book_epoch(std::vector<uint8_t>& b, int epochNumber, int C, int N, const float* samples, int cap,
+                const double* atoms, const int* counts) {
+    const size_t dataPos = b.size();
+    put_u8(b, 7);
+    put_u32(b, 0);
+    put_u16(b, (unsigned)epochNumber);
+    put_u32(b, (uint32_t)N);
+    for (int c = 0; c < C; ++c) {
+        put_u8(b, 8);
+        put_u32(b, (uint32_t)(2 + 4 * (size_t)N));
+        put_u16(b, (unsigned)(c + 1));
+        for (int i = 0; i < N; ++i) put_f32(b, samples[(size_t)c * N + i]);
+        const size_t atomsPos = b.size();
+        put_u8(b, 9);
+        put_u32(b, 0);
+        put_u16(b, (unsigned)(c + 1));
+        const int n = std::min(counts[c], cap);
+        for (int a = 0; a < n; ++a) {
+            put_u8(b, 13);  // ATOM_GABOR
+            put_u8(b, 24);  // six float32 params
+            for (int p = 0; p < 6; ++p) put_f32(b, atoms[((size_t)c * cap + a) * 6 + p]);
+        }
+        set_u32(b, atomsPos + 1, (uint32_t)(b.size() - atomsPos - 5));
+    }
+    set_u32(b, dataPos + 1, (uint32_t)(b.size() - dataPos - 5));
+}
+
+void write_file(const std::string& path, const std::vector<uint8_t>& bytes, bool append) {
+    FILE* f = fopen(path.c_str(), append ? "ab" : "wb");
+    if (!f) throw Error(EMPI_ERR_IO, "couldNotCreateOutputFile");
+    if (!bytes.empty() && fwrite(bytes.data(), 1, bytes.size(), f) != bytes.size()) {
+        fclose(f);
+        throw Error(EMPI_ERR_IO, "couldNotWriteOutputFile");
+    }
+    fclose(f);
+}
+
+void check(empi_status st) {
+    if (st != EMPI_OK) throw Error(st, empi_last_error()[0] ? empi_last_error() : empi_status_string(st));
+}
+
+// The empi() body, src/empi.cpp:49-167.
+void run_config(const char* configPath, const empi_engine_opts* opts) {
+    Configuration conf;
+    conf.parse(configPath);
+    const double energyError = atof(conf.at("energyError").c_str());
+    if (energyError <= 0.0 || energyError >= 1.0) throw Error(EMPI_ERR_CONFIG, "invalidEnergyErrorValue");
+    empi_dictionary dict;
+    dict.energy_error = energyError;
+    dict.scale_min = conf.has("minAtomScale") ? atof(conf.at("minAtomScale").c_str()) : 0.0;
+    dict.scale_max = conf.has("maxAtomScale") ? atof(conf.at("maxAtomScale").c_str()) : INFINITY;
+    dict.freq_max = conf.has("maxAtomFrequency") ? atof(conf.at("maxAtomFrequency").c_str()) : INFINITY;
+    empi_settings settings;
+    settings.iteration_max = atoi(conf.at("maximalNumberOfIterations").c_str());
+    if (settings.iteration_max <= 0) throw Error(EMPI_ERR_CONFIG, "invalidMaximalNumberOfIterations");
+    settings.residual_energy = 1 - 0.01 * atof(conf.at("energyPercent").c_str());
+    if (settings.residual_energy < 0 || settings.residual_energy >= 1.0)
+        throw Error(EMPI_ERR_CONFIG, "invalidEnergyPercentValue");
+
+    const std::string& signalPath = conf.at("nameOfDataFile");
+    std::unique_ptr<SignalReader> reader;
+    if (conf.has("numberOfSamplesInEpoch")) {
+        int epochSize = atoi(conf.at("numberOfSamplesInEpoch").c_str());
+        if (epochSize <= 0) throw Error(EMPI_ERR_CONFIG, "invalidNumberOfSamplesInEpoch");
+        if (conf.has("selectedEpochs")) {
+            std::vector<int> epochs = parse_subset(conf.at("selectedEpochs"), INT_MAX / epochSize);
+            reader.reset(new SignalReader(signalPath, 1, epochSize, epochs));
+        } else {
+            reader.reset(new SignalReader(signalPath, 0, epochSize, {}));
+        }
+    } else {
+        if (conf.has("selectedEpochs")) conf.at("numberOfSamplesInEpoch");
+        reader.reset(new SignalReader(signalPath, 2, 0, {}));
+    }
+    reader->freqSampling = atof(conf.at("samplingFrequency").c_str());
+    if (reader->freqSampling <= 0.0) throw Error(EMPI_ERR_CONFIG, "invalidSamplingFrequency");
+    reader->channelCount = atoi(conf.at("numberOfChannels").c_str());
+    if (reader->channelCount <= 0) throw Error(EMPI_ERR_CONFIG, "invalidNumberOfChannels");
+    reader->selectedChannels = parse_subset(conf.at("selectedChannels"), reader->channelCount);
+
+    const int C = (int)reader->selectedChannels.size();
+    std::string typeOfMP = conf.at("MP");
+    std::transform(typeOfMP.begin(), typeOfMP.end(), typeOfMP.begin(), ::tolower);
+    empi_variant variant;
+    if (C == 1 || typeOfMP == "smp") variant = EMPI_SMP;
+    else if (typeOfMP == "mmp1") variant = EMPI_MMP1;
+    else if (typeOfMP == "mmp2") variant = EMPI_MMP2;
+    else if (typeOfMP == "mmp3") variant = EMPI_MMP3;
+    else throw Error(EMPI_ERR_CONFIG, "unsupportedDecompositionType");
+
+    std::string prefix = reader->path;
+    std::string::size_type slash = prefix.find_last_of('/');
+    if (slash != std::string::npos) prefix = prefix.substr(slash + 1);
+    prefix = prefix.substr(0, prefix.find_last_of('.'));
+    typeOfMP.resize(3);
+    const std::string bookPath = conf.at("nameOfOutputDirectory") + "/" + prefix + "_" + typeOfMP + ".b";
+    write_file(bookPath, {}, false);  // BookWriter opens (truncates) the file up front
+
+    // read every epoch first; a read error ends the job after the epochs
+    // before it are decomposed and written, as in the reference's loop
+    std::vector<std::vector<float>> epochs;
+    int N = 0;
+    std::unique_ptr<Error> pending;
+    try {
+        for (;;) {
+            int count = 0;
+            std::vector<float> e = reader->read(count);
+            if (!count) break;
+            if (epochs.empty()) N = count;
+            if (count != N) throw Error(EMPI_ERR_IO, "fileIsTruncated");
+            epochs.push_back(std::move(e));
+        }
+    } catch (const Error& e) {
+        pending.reset(new Error(e));
+    }
+
+    std::vector<uint8_t> book;
+    if (!epochs.empty()) {
+        empi_engine* eng = nullptr;
+        check(empi_engine_create(opts, &eng));
+        std::unique_ptr<empi_engine, void (*)(empi_engine*)> eg(eng, empi_engine_destroy);
+        std::vector<empi_epoch> eps;
+        for (auto& e : epochs) eps.push_back(empi_epoch{reader->freqSampling, C, N, e.data()});
+        empi_batch* batch = nullptr;
+        check(empi_batch_create(eng, variant, &dict, &settings, eps.data(), (int)eps.size(), &batch));
+        std::unique_ptr<empi_batch, void (*)(empi_batch*)> bg(batch, empi_batch_destroy);
+        check(empi_batch_load(batch, eps.data()));
+        check(empi_batch_run(batch));
+        uint64_t atomCount = 0;
+        check(empi_dictionary_size(&dict, reader->freqSampling, N, &atomCount, nullptr));
+        const int cap = settings.iteration_max;
+        const bool smp = variant == EMPI_SMP;
+        const int loops = smp ? C : 1;
+        std::vector<double> atoms((size_t)C * cap * 6), energies((size_t)loops * cap), totals(loops);
+        std::vector<int> counts(C);
+        std::vector<float> chanMajor((size_t)C * N);
+        for (size_t e = 0; e < epochs.size(); ++e) {
+            check(empi_batch_atoms(batch, (int)e, cap, atoms.data(), counts.data(), energies.data(), nullptr));
+            check(empi_batch_total_energy(batch, (int)e, totals.data()));
+            // src/empi.cpp:159 and src/classes.cpp:41-48
+            std::cout << "START" << '\t' << (e + 1) << '\t' << C << '\t' << settings.iteration_max << '\t'
+                      << 100 * (1 - settings.residual_energy) << std::endl;
+            for (int l = 0; l < loops; ++l) {
+                if (smp) std::cout << "CHANNEL\t" << l << std::endl;
+                const int n = counts[smp ? l : 0];
+                double residue = totals[l];
+                for (int it = 1; it <= n; ++it) {
+                    double energyProgress = 100.0 * (1.0 - residue / totals[l]);
+                    double totalProgress =
+                        std::max(100.0 * (it - 1) / settings.iteration_max, energyProgress);
+                    std::cout << "ATOM\t" << (it - 1) << '\t' << atomCount << '\t' << energyProgress << '\t'
+                              << totalProgress << std::endl;
+                    residue = energies[(size_t)l * cap + it - 1];
+                }
+            }
+            for (int c = 0; c < C; ++c)
+                for (int i = 0; i < N; ++i) chanMajor[(size_t)c * N + i] = epochs[e][(size_t)i * C + c];
+            if (e == 0) book_header(book, C, reader->freqSampling);
+            book_epoch(book, (int)e + 1, C, N, chanMajor.data(), cap, atoms.data(), counts.data());
+        }
+    }
+    write_file(bookPath, book, false);
+    if (pending) throw *pending;
+    puts(" END");
+}
+
+}  // namespace
+
+extern "C" empi_status empi_run_config(const char* config_path, const empi_engine_opts* opts) {
+    if (!config_path) return empi::fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    try {
+        run_config(config_path, opts);
+    } catch (const Error& e) {
+        return empi::fail(e.status, e.what());
+    } catch (const std::bad_alloc&) {
+        return empi::fail(EMPI_ERR_OUT_OF_MEMORY, "insufficientMemory");
+    } catch (...) {
+        return empi::fail(EMPI_ERR_INTERNAL, "internalError");
+    }
+    return empi::ok();
+}
+
+extern "C" empi_status empi_book_write(const char* path, int append, int epoch_number, double fs, int channels,
+                                       int n, const float* samples, int cap, const double* atoms,
+                                       const int* counts) {
+    if (!path || channels <= 0 || n < 0 || (n > 0 && !samples) || !counts)
+        return empi::fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    try {
+        std::vector<uint8_t> b;
+        if (!append) book_header(b, channels, fs);
+        book_epoch(b, epoch_number, channels, n, samples, cap, atoms, counts);
+        write_file(path, b, append != 0);
+    } catch (const Error& e) {
+        return empi::fail(e.status, e.what());
+    }
+    return empi::ok();
+}

@@ -1,0 +1,1249 @@
+// sm_100a kernels of the Matching Pursuit loop.
+//
+// Per MP iteration the device runs (all launches captured in a CUDA graph):
+//   k_cand_slots  slots whose FP32 max lies within the candidate band of the
+//                 instance's best (reads the tournament tree top-down)
+//   k_refresh<COLLECT>  FP32 recompute of those slots, emitting every bin in
+//                 the band
+//   k_rescore     FP64 direct DFT of each candidate bin, per channel
+//   k_select      FP64 energy (the reference formula) -> argmax -> atom params
+//   k_subtract    FP64 atom subtraction on the residual + channel energies
+//   k_sched_a/b   stop test, dirty t-range per scale, work-unit prefix sums
+//   k_refresh     windowed FFT + energies + per-slot max over the dirty range
+//   k_tree        leaf-chunk maxima for the chunks the refresh touched
+//   k_root        per-instance maximum over chunk maxima
+// Waits are never spun on: ordering comes from kernel boundaries only.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include "fft.cuh"
+#include "plan.hpp"
+
+namespace empi {
+
+enum Mode { MODE_SINGLE = 0, MODE_MMP1 = 1, MODE_MMP3 = 3 };
+
+enum Counter {
+    CTR_UNITS = 0,       // refresh work-queue head
+    CTR_TREE = 1,        // tree work-queue head
+    CTR_CSLOTS = 2,      // candidate slots emitted
+    CTR_CSLOT_Q = 3,     // candidate-slot work-queue head
+    CTR_CBINS = 4,       // candidate bins emitted
+    CTR_RESCORE_Q = 5,   // rescore work-queue head
+    CTR_TOTAL_UNITS = 6,
+    CTR_TOTAL_CHUNKS = 7,
+    CTR_ACTIVE = 8,      // instances still running after the last schedule
+    CTR_STAT_UNITS = 9,  // running totals for statistics
+    CTR_STAT_SLOTS = 10,
+    CTR_STAT_BINS = 11,
+    CTR_COUNT = 16
+};
+
+enum Status { ST_RUNNING = 0, ST_DONE = 1, ST_ERROR = 2 };
+enum ErrCode { ERR_NONE = 0, ERR_SIGNAL_EMPTY = 4, ERR_MAP_EMPTY = 5, ERR_CAND_OVERFLOW = 7 };
+
+struct InstPlan {
+    int dict, C, epoch, chan0;     // chan0: input channel (SMP) / -1 all / -2 sum (MMP2)
+    int ij_off, cen_off, pad0, pad1;
+    long long res_off, slot_off, chunk_off, out_off, in_off;
+    int in_channels, pad2;
+};
+
+struct InstState {
+    int status, it, err, nbins;
+    double etotal, eres;
+    unsigned long long best32;
+};
+
+struct CandSlot {
+    int inst, j, t, g;
+};
+
+struct CandBin {
+    int inst, j, t, k;
+    float e32;
+    int pad;
+    double e64;
+};
+
+struct WinMeta {
+    double c64, fst0;
+    int iL, W, ci;
+    float cf;
+};
+
+struct BatchDev {
+    const ScalePlan* scales;
+    const DictPlan* dicts;
+    const InstPlan* insts;
+    const int2* blk_ic;   // (instance, channel) of each per-channel block
+    const float2* tw;     // exp(-2 pi i m / kTwN)
+    const float* input;   // all epochs, float32 interleaved
+    int ninst, nblk_ic, cmax, iter_max, mode;
+    double residual_energy;
+    float band;
+    int cslot_cap, cbin_cap, inst_bin_cap;
+    double* residual;
+    InstState* state;
+    unsigned long long* slots;
+    unsigned long long* chunks;
+    int2* dirty;        // per (i, j): t range [x, y]
+    int* ij_units;      // per (i, j): exclusive unit prefix within instance (nscales + 1 per inst)
+    int* ij_chunks;     // per (i, j): exclusive dirty-chunk prefix (nscales + 1 per inst)
+    int2* ij_crange;    // per (i, j): first dirty chunk, count
+    int* inst_units;    // exclusive prefix over instances (ninst + 1)
+    int* inst_chunks;   // exclusive prefix over instances (ninst + 1)
+    int* ctr;
+    CandSlot* cslots;
+    CandBin* cbins;
+    double2* cbin_v;    // cbin_cap x cmax
+    int* inst_bins;     // ninst x inst_bin_cap bin ids
+    double* atoms;      // per instance: iter_max x C x 6
+    double* energies;   // ninst x iter_max
+    int4* indices;      // ninst x iter_max: (scale, t, f, -)
+    double* chan_energy;  // per (instance, channel)
+    double* stats;        // [0] reference-equivalent FFT flops, [1] algorithmic bytes, [2] slots
+    float* dump;          // optional energy-map dump [f][t] of one scale
+};
+
+// ------------------------------------------------------------ helpers
+
+__device__ __forceinline__ unsigned long long pack_key(float e, unsigned low) {
+    if (!(e >= 0.0f && e <= 3.0e38f)) e = 0.0f;
+    return ((unsigned long long)__float_as_uint(e) << 32) | (unsigned long long)low;
+}
+
+// t grid, src/gabor.cpp:262-264 (t = ti * tMax / (tCount - 1))
+__device__ __forceinline__ double grid_t(int ti, double tMax, int tcount) {
+    return __ddiv_rn(__dmul_rn((double)ti, tMax), (double)(tcount - 1));
+}
+
+// window bounds, src/gabor.cpp:284-286
+__device__ __forceinline__ void window_bounds(double t0, double hw, double fs, int N, int& iL, int& iR,
+                                              double& t0fixed) {
+    long long l = __double2ll_rn(__dmul_rn(__dsub_rn(t0, hw), fs));
+    long long r = __double2ll_rn(__dmul_rn(__dadd_rn(t0, hw), fs));
+    iL = (int)(l > 0 ? l : 0);
+    iR = (int)(r < (long long)N - 1 ? r : (long long)N - 1);
+    t0fixed = __dsub_rn(t0, __ddiv_rn((double)iL, fs));
+}
+
+// refresh rule |t - tA| <= (s + sA) * 3, src/gabor.cpp:204
+__device__ __forceinline__ bool touches(int ti, double tMax, int tcount, double tA, double lim) {
+    return fabs(__dsub_rn(grid_t(ti, tMax, tcount), tA)) <= lim;
+}
+
+__device__ __forceinline__ void dirty_range(const ScalePlan& sp, double tMax, double tA, double sA, int& lo,
+                                            int& hi) {
+    const double lim = __dmul_rn(__dadd_rn(sp.s, sA), 3.0);
+    const int tc = sp.tcount;
+    const double dt = tMax / (tc - 1);
+    double a = floor((tA - lim) / dt) - 2.0, c = ceil((tA + lim) / dt) + 2.0;
+    int g0 = (int)fmax(0.0, fmin((double)(tc - 1), a));
+    int g1 = (int)fmax(0.0, fmin((double)(tc - 1), c));
+    lo = g0;
+    while (lo > 0 && touches(lo - 1, tMax, tc, tA, lim)) --lo;
+    while (lo <= g1 && !touches(lo, tMax, tc, tA, lim)) ++lo;
+    hi = g1;
+    while (hi < tc - 1 && touches(hi + 1, tMax, tc, tA, lim)) ++hi;
+    while (hi >= lo && !touches(hi, tMax, tc, tA, lim)) --hi;
+    if (lo > hi) {
+        lo = 0;
+        hi = -1;
+    }
+}
+
+__device__ __forceinline__ int group_units(int n, int g, const ScalePlan& sp) {
+    const int B = g >= 2 ? sp.B2 : sp.B1;
+    return (n + B - 1) / B;
+}
+
+__device__ __forceinline__ int upper_index(const int* prefix, int n, int u) {
+    // largest i in [0, n) with prefix[i] <= u (prefix non-decreasing, prefix[0] = 0)
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(prefix + mid) <= u) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// exp(-2 pi i a / b) for integers a < b (b a power of two)
+__device__ __forceinline__ float2 twiddle_frac(long long a, long long b, const float2* tw) {
+    if (b <= kTwN) return __ldg(tw + a * (kTwN / b));
+    float s, c;
+    sincospif(-2.0f * (float)a / (float)b, &s, &c);
+    return make_float2(c, s);
+}
+
+// Energy of one channel's spectral value X (unnormalised FFT bin) at bin k:
+// fs |v|^2 normReal^2 with v = X e^{i theta_k} / fs, GaborComputer::compute
+// (src/gabor.cpp:54-71) in closed form: K |X|^4 / (|X|^2 + e Re(X^2 e^{i psi})).
+__device__ __forceinline__ float phase_turns(int k, const ScalePlan& sp, const WinMeta& m, bool high) {
+    double tt = 2.0 * (double)k * m.c64 / (double)sp.nfft;
+    if (high) tt -= m.fst0;
+    tt -= rint(tt);
+    return (float)tt;
+}
+
+__device__ __forceinline__ float exp_factor(int k, const ScalePlan& sp, double fs, bool high) {
+    double f = (double)k * fs / (double)sp.nfft;
+    double f4 = high ? (0.5 * fs - f) : f;
+    return (float)exp(-2 * CUDART_PI * sp.s * sp.s * f4 * f4);
+}
+
+__device__ __forceinline__ float energy_one(float2 X, int k, const ScalePlan& sp, const WinMeta& m, double fs) {
+    const float p = X.x * X.x + X.y * X.y;
+    if (k < sp.klo || k > sp.khi) {
+        const bool high = k >= sp.khf;
+        const float e = exp_factor(k, sp, fs, high);
+        float sn, cs;
+        sincospif(2.0f * phase_turns(k, sp, m, high), &sn, &cs);
+        const float re = (X.x * X.x - X.y * X.y) * cs - 2.0f * X.x * X.y * sn;
+        const float D = p + e * re;
+        return (D > 0.0f && p > 0.0f) ? sp.Kc * p * (p / D) : 0.0f;
+    }
+    return sp.Kc * p;
+}
+
+// MMP1 closed form (constraint + normalisation, src/mmp.cpp:9-21 with
+// src/gabor.cpp:54-71) from P = sum |X_c|^2 and S = sum X_c^2.
+__device__ __forceinline__ float energy_mmp1(float P, float2 S, int k, const ScalePlan& sp, const WinMeta& m,
+                                             double fs) {
+    const float as = sqrtf(S.x * S.x + S.y * S.y);
+    if (k < sp.klo || k > sp.khi) {
+        const float e = exp_factor(k, sp, fs, false);
+        if (as == 0.0f) return sp.K1 * P / (1.0f + e);
+        float sn, cs;
+        sincospif(2.0f * phase_turns(k, sp, m, false), &sn, &cs);
+        const float re = S.x * cs - S.y * sn;
+        const float D = as + e * re;
+        return D > 0.0f ? sp.K1 * (P + as) * (as / D) : 0.0f;
+    }
+    return sp.K1 * (P + as);
+}
+
+// Segmented max over consecutive lanes that share a window, then one shared
+// atomic per segment head.
+__device__ __forceinline__ void seg_max_flush(unsigned long long key, int w, unsigned long long* wkey) {
+    const unsigned lane = threadIdx.x & 31;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        unsigned long long ok = __shfl_down_sync(0xffffffffu, key, off);
+        int ow = __shfl_down_sync(0xffffffffu, w, off);
+        if (lane + off < 32 && ow == w && ok > key) key = ok;
+    }
+    int pw = __shfl_up_sync(0xffffffffu, w, 1);
+    if (w >= 0 && (lane == 0 || pw != w)) atomicMax(wkey + w, key);
+}
+
+// ------------------------------------------------------------ refresh
+
+constexpr int kVPT = kUnitPoints / kUnitThreads;
+constexpr int kBufFloat2 = kUnitPoints + kUnitPoints / 16 + 16;
+constexpr int kAccBins = kUnitPoints + kMaxWindowsPerUnit;
+
+template <int MODE>
+constexpr size_t refresh_smem_bytes() {
+    return sizeof(float2) * kBufFloat2 + sizeof(WinMeta) * kMaxWindowsPerUnit +
+           sizeof(unsigned long long) * kMaxWindowsPerUnit +
+           (MODE == MODE_SINGLE ? 0 : sizeof(float) * kAccBins * (MODE == MODE_MMP1 ? 3 : 1));
+}
+
+template <int MODE, bool COLLECT>
+__device__ void process_unit(const BatchDev& b, unsigned char* smem, int inst, int j, int g, int t_start,
+                             int nwin, unsigned thr_bits) {
+    float2* buf = reinterpret_cast<float2*>(smem);
+    WinMeta* meta = reinterpret_cast<WinMeta*>(smem + sizeof(float2) * kBufFloat2);
+    unsigned long long* wkey = reinterpret_cast<unsigned long long*>(
+        smem + sizeof(float2) * kBufFloat2 + sizeof(WinMeta) * kMaxWindowsPerUnit);
+    float* acc = reinterpret_cast<float*>(smem + sizeof(float2) * kBufFloat2 + sizeof(WinMeta) * kMaxWindowsPerUnit +
+                                          sizeof(unsigned long long) * kMaxWindowsPerUnit);
+
+    const InstPlan ip = b.insts[inst];
+    const DictPlan dp = b.dicts[ip.dict];
+    const ScalePlan sp = b.scales[dp.scale0 + j];
+    const double fs = dp.fs;
+    const int L = sp.L, logL = sp.logL, M = sp.M, F = sp.F;
+    const int Nh = sp.nfft >> 1;
+    const bool pair = g >= 2;
+    const int nf = pair ? 2 : 1;
+    const int nb = g == 0 ? L + 1 : (pair ? 2 * L : L);
+    const int r = g == 0 ? 0 : (g == 1 ? M / 2 : g - 1);
+    const int tid = threadIdx.x, T = blockDim.x;
+
+    for (int w = tid; w < nwin; w += T) {
+        const int ti = t_start + w;
+        const double t0 = grid_t(ti, dp.tMax, sp.tcount);
+        int iL, iR;
+        double t0fixed;
+        window_bounds(t0, sp.hw, fs, dp.N, iL, iR, t0fixed);
+        WinMeta m;
+        m.c64 = t0fixed * fs;
+        m.fst0 = fs * t0;
+        m.iL = iL;
+        m.W = iR - iL + 1;
+        const double cfl = floor(m.c64);
+        m.ci = (int)cfl;
+        m.cf = (float)(m.c64 - cfl);
+        meta[w] = m;
+        wkey[w] = 0ull;
+    }
+    // W_Nfft^rho for the residues of this group
+    float2 wr0, wr1 = make_float2(1.f, 0.f);
+    {
+        float s0, c0;
+        sincospif(-2.0f * (float)r / (float)sp.nfft, &s0, &c0);
+        wr0 = make_float2(c0, s0);
+        if (pair) {
+            sincospif(-2.0f * (float)(M - r) / (float)sp.nfft, &s0, &c0);
+            wr1 = make_float2(c0, s0);
+        }
+    }
+    const int nbins = nwin * nb;
+    if (MODE != MODE_SINGLE) {
+        for (int i = tid; i < nbins * (MODE == MODE_MMP1 ? 3 : 1); i += T) acc[i] = 0.0f;
+    }
+    __syncthreads();
+
+    const int twL = kTwN >> logL;          // table stride for W_L
+    const int tw2L = (kTwN / 2) >> logL;   // table stride for W_{2L}
+    for (int c = 0; c < ip.C; ++c) {
+        const double* x = b.residual + ip.res_off + (long long)c * dp.N;
+        // load: y_r[n'] = sum_m z[n' + mL] W_Nh^{r (n' + mL)}, z[n] = x[2n] g(2n) + i x[2n+1] g(2n+1)
+        const int total = nwin << logL;
+        for (int idx = tid; idx < total; idx += T) {
+            const int w = idx >> logL;
+            const int np = idx & (L - 1);
+            const WinMeta m = meta[w];
+            float2 a1 = make_float2(0.f, 0.f), a2 = make_float2(0.f, 0.f);
+            for (int mm = 0; mm < F; ++mm) {
+                const int n = np + mm * L;
+                const int i0 = 2 * n;
+                if (i0 >= m.W) break;
+                const float x0 = (float)__ldg(x + m.iL + i0);
+                const float x1 = (i0 + 1 < m.W) ? (float)__ldg(x + m.iL + i0 + 1) : 0.0f;
+                const float d0 = (float)(i0 - m.ci) - m.cf;
+                const float y0 = d0 * sp.aG, y1 = (d0 + 1.0f) * sp.aG;
+                const float2 z = make_float2(x0 * expf(-y0 * y0), x1 * expf(-y1 * y1));
+                if (r == 0) {
+                    a1 = cadd(a1, z);
+                } else {
+                    const long long rn = ((long long)r * n) & (Nh - 1);
+                    const float2 tw = twiddle_frac(rn, Nh, b.tw);
+                    a1 = cadd(a1, cmul(z, tw));
+                    if (pair) a2 = cadd(a2, cmulc(z, tw));
+                }
+            }
+            buf[pad16(((w * nf) << logL) + np)] = a1;
+            if (pair) buf[pad16(((w * nf + 1) << logL) + np)] = cmul(a2, __ldg(b.tw + np * twL));
+        }
+        __syncthreads();
+        fft_batch<kVPT, kTwN>(buf, logL, (nwin * nf) << logL, b.tw);
+
+        // post: X[k] = (A + conj(B))/2 - i W_Nfft^k (A - conj(B))/2
+        for (int base = 0; base < nbins; base += T) {
+            const int idx = base + tid;
+            int w = -1, k = 0;
+            float2 X = make_float2(0.f, 0.f);
+            if (idx < nbins) {
+                w = idx / nb;
+                const int jb = idx - w * nb;
+                int q, rho;
+                float2 A, Bq, wr;
+                if (g == 0) {
+                    q = jb;
+                    const int o = w << logL;
+                    A = buf[pad16(o + (q & (L - 1)))];
+                    Bq = buf[pad16(o + ((L - q) & (L - 1)))];
+                    rho = 0;
+                    wr = make_float2(1.f, 0.f);
+                } else if (g == 1) {
+                    q = jb;
+                    const int o = w << logL;
+                    A = buf[pad16(o + q)];
+                    Bq = buf[pad16(o + L - 1 - q)];
+                    rho = M / 2;
+                    wr = wr0;
+                } else {
+                    const int o0 = (2 * w) << logL, o1 = (2 * w + 1) << logL;
+                    if (jb < L) {
+                        q = jb;
+                        A = buf[pad16(o0 + q)];
+                        Bq = buf[pad16(o1 + L - 1 - q)];
+                        rho = r;
+                        wr = wr0;
+                    } else {
+                        q = jb - L;
+                        A = buf[pad16(o1 + q)];
+                        Bq = buf[pad16(o0 + L - 1 - q)];
+                        rho = M - r;
+                        wr = wr1;
+                    }
+                }
+                k = M * q + rho;
+                if (k < sp.fcount) {
+                    const float2 wk = cmul(wr, __ldg(b.tw + q * tw2L));
+                    const float2 Bc = make_float2(Bq.x, -Bq.y);
+                    const float2 E = make_float2(0.5f * (A.x + Bc.x), 0.5f * (A.y + Bc.y));
+                    const float2 D = make_float2(0.5f * (A.x - Bc.x), 0.5f * (A.y - Bc.y));
+                    const float2 O = make_float2(D.y, -D.x);  // -i D
+                    X = cadd(E, cmul(wk, O));
+                } else {
+                    k = -1;
+                }
+            }
+            if (MODE == MODE_SINGLE) {
+                float e = 0.0f;
+                if (k >= 0 && w >= 0) e = energy_one(X, k, sp, meta[w], fs);
+                const unsigned long long key = (k >= 0 && w >= 0) ? pack_key(e, (unsigned)k) : 0ull;
+                if (!COLLECT && b.dump && k >= 0 && w >= 0) b.dump[(long long)k * sp.tcount + t_start + w] = e;
+                if (COLLECT) {
+                    if (k >= 0 && w >= 0 && __float_as_uint(e) >= thr_bits) {
+                        const int slot = atomicAdd(b.ctr + CTR_CBINS, 1);
+                        if (slot < b.cbin_cap) {
+                            const int li = atomicAdd(&b.state[inst].nbins, 1);
+                            if (li < b.inst_bin_cap) {
+                                CandBin cb;
+                                cb.inst = inst;
+                                cb.j = j;
+                                cb.t = t_start + w;
+                                cb.k = k;
+                                cb.e32 = e;
+                                cb.pad = 0;
+                                cb.e64 = 0.0;
+                                b.cbins[slot] = cb;
+                                b.inst_bins[(long long)inst * b.inst_bin_cap + li] = slot;
+                            } else {
+                                b.state[inst].err = ERR_CAND_OVERFLOW;
+                            }
+                        } else {
+                            b.state[inst].err = ERR_CAND_OVERFLOW;
+                        }
+                    }
+                } else {
+                    seg_max_flush(key, w, wkey);
+                }
+            } else if (k >= 0 && w >= 0) {
+                if (MODE == MODE_MMP3 || k >= sp.khf) {
+                    acc[idx] += energy_one(X, k, sp, meta[w], fs);
+                } else {
+                    acc[idx] += X.x * X.x + X.y * X.y;
+                    acc[nbins + idx] += X.x * X.x - X.y * X.y;
+                    acc[2 * nbins + idx] += 2.0f * X.x * X.y;
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    if (MODE != MODE_SINGLE) {
+        for (int base = 0; base < nbins; base += T) {
+            const int idx = base + tid;
+            int w = -1, k = -1;
+            float e = 0.0f;
+            if (idx < nbins) {
+                w = idx / nb;
+                const int jb = idx - w * nb;
+                int q, rho;
+                if (g == 0) {
+                    q = jb;
+                    rho = 0;
+                } else if (g == 1) {
+                    q = jb;
+                    rho = M / 2;
+                } else if (jb < L) {
+                    q = jb;
+                    rho = r;
+                } else {
+                    q = jb - L;
+                    rho = M - r;
+                }
+                k = M * q + rho;
+                if (k >= sp.fcount) k = -1;
+                if (k >= 0) {
+                    if (MODE == MODE_MMP3 || k >= sp.khf) {
+                        e = acc[idx];
+                    } else {
+                        e = energy_mmp1(acc[idx], make_float2(acc[nbins + idx], acc[2 * nbins + idx]), k, sp,
+                                        meta[w], fs);
+                    }
+                }
+            }
+            if (COLLECT) {
+                if (k >= 0 && __float_as_uint(e) >= thr_bits) {
+                    const int slot = atomicAdd(b.ctr + CTR_CBINS, 1);
+                    if (slot < b.cbin_cap) {
+                        const int li = atomicAdd(&b.state[inst].nbins, 1);
+                        if (li < b.inst_bin_cap) {
+                            CandBin cb;
+                            cb.inst = inst;
+                            cb.j = j;
+                            cb.t = t_start + w;
+                            cb.k = k;
+                            cb.e32 = e;
+                            cb.pad = 0;
+                            cb.e64 = 0.0;
+                            b.cbins[slot] = cb;
+                            b.inst_bins[(long long)inst * b.inst_bin_cap + li] = slot;
+                        } else {
+                            b.state[inst].err = ERR_CAND_OVERFLOW;
+                        }
+                    } else {
+                        b.state[inst].err = ERR_CAND_OVERFLOW;
+                    }
+                }
+            } else {
+                const unsigned long long key = k >= 0 ? pack_key(e, (unsigned)k) : 0ull;
+                if (b.dump && k >= 0) b.dump[(long long)k * sp.tcount + t_start + w] = e;
+                seg_max_flush(key, k >= 0 ? w : -1, wkey);
+            }
+        }
+        __syncthreads();
+    }
+
+    if (!COLLECT) {
+        unsigned long long* out = b.slots + ip.slot_off + sp.slot_base;
+        for (int w = tid; w < nwin; w += T) out[(long long)(t_start + w) * sp.G + g] = wkey[w];
+    }
+    __syncthreads();
+}
+
+// Persistent refresh: CTAs pull (instance, scale, group, t-batch) units from
+// the schedule's prefix sums; COLLECT pulls candidate slots instead.
+template <int MODE, bool COLLECT>
+__global__ void __launch_bounds__(kUnitThreads, 1) k_refresh(BatchDev b) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_unit;
+    const int total = COLLECT ? min(b.ctr[CTR_CSLOTS], b.cslot_cap) : b.ctr[CTR_TOTAL_UNITS];
+    for (;;) {
+        if (threadIdx.x == 0) s_unit = atomicAdd(b.ctr + (COLLECT ? CTR_CSLOT_Q : CTR_UNITS), 1);
+        __syncthreads();
+        const int u = s_unit;
+        __syncthreads();
+        if (u >= total) break;
+        if (COLLECT) {
+            const CandSlot cs = b.cslots[u];
+            const unsigned best = (unsigned)(b.state[cs.inst].best32 >> 32);
+            const float thr = __uint_as_float(best) * (1.0f - b.band);
+            process_unit<MODE, true>(b, smem, cs.inst, cs.j, cs.g, cs.t, 1, __float_as_uint(thr));
+        } else {
+            const int inst = upper_index(b.inst_units, b.ninst, u);
+            int rem = u - b.inst_units[inst];
+            const InstPlan ip = b.insts[inst];
+            const DictPlan dp = b.dicts[ip.dict];
+            const int j = upper_index(b.ij_units + ip.ij_off + inst, dp.nscales, rem);
+            rem -= b.ij_units[ip.ij_off + inst + j];
+            const ScalePlan sp = b.scales[dp.scale0 + j];
+            const int2 dr = b.dirty[ip.ij_off + j];
+            const int n = dr.y - dr.x + 1;
+            int g = 0;
+            for (; g < sp.G; ++g) {
+                const int ng = group_units(n, g, sp);
+                if (rem < ng) break;
+                rem -= ng;
+            }
+            const int B = g >= 2 ? sp.B2 : sp.B1;
+            const int t_start = dr.x + rem * B;
+            const int nwin = min(B, dr.y - t_start + 1);
+            process_unit<MODE, false>(b, smem, inst, j, g, t_start, nwin, 0u);
+        }
+    }
+}
+
+// ------------------------------------------------------------ schedule
+
+enum SchedMode { SCHED_ITERATE = 0, SCHED_INIT = 1, SCHED_ATOM = 2 };
+
+// One CTA per instance.  SCHED_INIT: every window dirty (only_scale >= 0
+// restricts it to one scale).  SCHED_ITERATE: stop test on the residual energy
+// of the previous subtraction (src/classes.cpp:67-70), then the dirty range of
+// every scale from the subtracted atom (src/gabor.cpp:197-208).  SCHED_ATOM:
+// dirty ranges of the atom (tA, sA) given by the caller.
+__global__ void k_sched_a(BatchDev b, int mode, int only_scale, double tA_in, double sA_in) {
+    const int init = mode == SCHED_INIT;
+    const int inst = blockIdx.x;
+    const InstPlan ip = b.insts[inst];
+    const DictPlan dp = b.dicts[ip.dict];
+    __shared__ int s_active;
+    __shared__ double s_tA, s_sA;
+    if (threadIdx.x == 0) {
+        InstState& st = b.state[inst];
+        int active = st.status == ST_RUNNING;
+        if (mode == SCHED_ATOM) {
+            s_tA = tA_in;
+            s_sA = sA_in;
+        } else if (active && init) {
+            double e = 0.0;
+            for (int c = 0; c < ip.C; ++c) e += b.chan_energy[ip.cen_off + c];
+            st.etotal = e;
+            st.eres = e;
+            if (e == 0.0) {
+                st.status = ST_ERROR;
+                st.err = ERR_SIGNAL_EMPTY;
+                active = 0;
+            }
+        } else if (active) {
+            double e = 0.0;
+            for (int c = 0; c < ip.C; ++c) e += b.chan_energy[ip.cen_off + c];
+            st.eres = e;
+            b.energies[(long long)inst * b.iter_max + st.it - 1] = e;
+            if (e / st.etotal <= b.residual_energy) {
+                st.status = ST_DONE;
+                active = 0;
+            } else {
+                const double* p = b.atoms + ip.out_off + (long long)(st.it - 1) * ip.C * 6;
+                s_tA = p[2] / dp.fs;
+                s_sA = p[3] / dp.fs;
+            }
+        }
+        s_active = active;
+    }
+    __syncthreads();
+    int* units = b.ij_units + ip.ij_off + inst;
+    int* chunks = b.ij_chunks + ip.ij_off + inst;
+    for (int j = threadIdx.x; j < dp.nscales; j += blockDim.x) {
+        const ScalePlan sp = b.scales[dp.scale0 + j];
+        int lo = 0, hi = -1;
+        if (s_active) {
+            if (init) {
+                if (only_scale < 0 || only_scale == j) {
+                    lo = 0;
+                    hi = sp.tcount - 1;
+                }
+            } else {
+                dirty_range(sp, dp.tMax, s_tA, s_sA, lo, hi);
+            }
+        }
+        b.dirty[ip.ij_off + j] = make_int2(lo, hi);
+        int nu = 0, nc = 0, c0 = 0;
+        if (hi >= lo) {
+            const int n = hi - lo + 1;
+            for (int g = 0; g < sp.G; ++g) nu += group_units(n, g, sp);
+            const long long s0 = sp.slot_base + (long long)lo * sp.G;
+            const long long s1 = sp.slot_base + (long long)(hi + 1) * sp.G - 1;
+            c0 = (int)(s0 / kChunk);
+            nc = (int)(s1 / kChunk) - c0 + 1;
+            // statistics: reference-equivalent FFT flops (2.5 Nfft log2 Nfft per
+            // window and channel) and compulsory bytes (the residual span read
+            // once per channel, one 8-byte slot write per (window, group))
+            int iL0, iR0, iL1, iR1;
+            double tf;
+            window_bounds(grid_t(lo, dp.tMax, sp.tcount), sp.hw, dp.fs, dp.N, iL0, iR0, tf);
+            window_bounds(grid_t(hi, dp.tMax, sp.tcount), sp.hw, dp.fs, dp.N, iL1, iR1, tf);
+            const double lg = log2((double)sp.nfft);
+            atomicAdd(b.stats + 0, (double)n * ip.C * 2.5 * sp.nfft * lg);
+            atomicAdd(b.stats + 1, 8.0 * ip.C * (double)(iR1 - iL0 + 1) + 8.0 * (double)n * sp.G);
+            atomicAdd(b.stats + 2, (double)n * sp.G);
+        }
+        units[j + 1] = nu;
+        chunks[j + 1] = nc;
+        b.ij_crange[ip.ij_off + j] = make_int2(c0, nc);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        units[0] = 0;
+        chunks[0] = 0;
+        for (int j = 0; j < dp.nscales; ++j) {
+            units[j + 1] += units[j];
+            chunks[j + 1] += chunks[j];
+        }
+    }
+}
+
+// Single CTA: exclusive scan of per-instance unit and chunk totals; resets the
+// work queues and candidate lists.
+__global__ void k_sched_b(BatchDev b) {
+    __shared__ int s_u[1024], s_c[1024], s_a[1024];
+    const int T = blockDim.x, tid = threadIdx.x;
+    const int per = (b.ninst + T - 1) / T;
+    const int i0 = tid * per, i1 = min(b.ninst, i0 + per);
+    int su = 0, sc = 0, sa = 0;
+    for (int i = i0; i < i1; ++i) {
+        const InstPlan ip = b.insts[i];
+        const int ns = b.dicts[ip.dict].nscales;
+        su += b.ij_units[ip.ij_off + i + ns];
+        sc += b.ij_chunks[ip.ij_off + i + ns];
+        sa += b.state[i].status == ST_RUNNING;
+    }
+    s_u[tid] = su;
+    s_c[tid] = sc;
+    s_a[tid] = sa;
+    __syncthreads();
+    for (int off = 1; off < T; off <<= 1) {
+        int vu = tid >= off ? s_u[tid - off] : 0;
+        int vc = tid >= off ? s_c[tid - off] : 0;
+        int va = tid >= off ? s_a[tid - off] : 0;
+        __syncthreads();
+        s_u[tid] += vu;
+        s_c[tid] += vc;
+        s_a[tid] += va;
+        __syncthreads();
+    }
+    int pu = tid ? s_u[tid - 1] : 0, pc = tid ? s_c[tid - 1] : 0;
+    for (int i = i0; i < i1; ++i) {
+        const InstPlan ip = b.insts[i];
+        const int ns = b.dicts[ip.dict].nscales;
+        b.inst_units[i] = pu;
+        b.inst_chunks[i] = pc;
+        pu += b.ij_units[ip.ij_off + i + ns];
+        pc += b.ij_chunks[ip.ij_off + i + ns];
+    }
+    if (tid == T - 1) {
+        b.inst_units[b.ninst] = s_u[T - 1];
+        b.inst_chunks[b.ninst] = s_c[T - 1];
+        b.ctr[CTR_TOTAL_UNITS] = s_u[T - 1];
+        b.ctr[CTR_TOTAL_CHUNKS] = s_c[T - 1];
+        b.ctr[CTR_ACTIVE] = s_a[T - 1];
+        b.ctr[CTR_STAT_UNITS] += s_u[T - 1];
+        b.ctr[CTR_UNITS] = 0;
+        b.ctr[CTR_TREE] = 0;
+        b.ctr[CTR_CSLOTS] = 0;
+        b.ctr[CTR_CSLOT_Q] = 0;
+        b.ctr[CTR_CBINS] = 0;
+        b.ctr[CTR_RESCORE_Q] = 0;
+    }
+}
+
+// ------------------------------------------------------------ tournament tree
+
+// Leaf chunks: max over kChunk slot keys, re-keyed by slot index.
+__global__ void k_tree(BatchDev b) {
+    const int lane = threadIdx.x & 31;
+    const int total = b.ctr[CTR_TOTAL_CHUNKS];
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(b.ctr + CTR_TREE, 1);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= total) break;
+        const int inst = upper_index(b.inst_chunks, b.ninst, item);
+        int rem = item - b.inst_chunks[inst];
+        const InstPlan ip = b.insts[inst];
+        const DictPlan dp = b.dicts[ip.dict];
+        const int j = upper_index(b.ij_chunks + ip.ij_off + inst, dp.nscales, rem);
+        rem -= b.ij_chunks[ip.ij_off + inst + j];
+        const int chunk = b.ij_crange[ip.ij_off + j].x + rem;
+        const long long s0 = (long long)chunk * kChunk;
+        const long long s1 = min(s0 + kChunk, dp.slots);
+        const unsigned long long* sl = b.slots + ip.slot_off;
+        unsigned long long best = 0;
+        for (long long s = s0 + lane; s < s1; s += 32) {
+            const unsigned long long v = sl[s];
+            const unsigned long long key = (v & 0xffffffff00000000ull) | (unsigned long long)(s);
+            best = key > best ? key : best;
+        }
+#pragma unroll
+        for (int off = 16; off; off >>= 1) {
+            unsigned long long o = __shfl_down_sync(0xffffffffu, best, off);
+            best = o > best ? o : best;
+        }
+        if (lane == 0) b.chunks[ip.chunk_off + chunk] = best;
+    }
+}
+
+__device__ __forceinline__ unsigned long long block_max_u64(unsigned long long v, unsigned long long* red) {
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+        unsigned long long o = __shfl_down_sync(0xffffffffu, v, off);
+        v = o > v ? o : v;
+    }
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0ull;
+#pragma unroll
+        for (int off = 16; off; off >>= 1) {
+            unsigned long long o = __shfl_down_sync(0xffffffffu, v, off);
+            v = o > v ? o : v;
+        }
+    }
+    __syncthreads();
+    return v;
+}
+
+// Root: per-instance best over chunk maxima.
+__global__ void k_root(BatchDev b) {
+    __shared__ unsigned long long red[32];
+    const int inst = blockIdx.x;
+    if (b.state[inst].status != ST_RUNNING) return;
+    const InstPlan ip = b.insts[inst];
+    const DictPlan dp = b.dicts[ip.dict];
+    unsigned long long best = 0;
+    for (int c = threadIdx.x; c < dp.chunks; c += blockDim.x) {
+        const unsigned long long v = b.chunks[ip.chunk_off + c];
+        best = v > best ? v : best;
+    }
+    best = block_max_u64(best, red);
+    if (threadIdx.x == 0) b.state[inst].best32 = best;
+}
+
+// ------------------------------------------------------------ candidates
+
+__device__ __forceinline__ void slot_to_jtg(const BatchDev& b, const DictPlan& dp, long long slot, int& j, int& t,
+                                            int& g) {
+    int lo = 0, hi = dp.nscales - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (b.scales[dp.scale0 + mid].slot_base <= slot) lo = mid;
+        else hi = mid - 1;
+    }
+    j = lo;
+    const ScalePlan sp = b.scales[dp.scale0 + j];
+    const long long rel = slot - sp.slot_base;
+    t = (int)(rel / sp.G);
+    g = (int)(rel - (long long)t * sp.G);
+}
+
+// One CTA per instance: every slot whose FP32 max is within the band of the
+// instance's best becomes a candidate (chunks first, then their slots).
+__global__ void k_cand_slots(BatchDev b) {
+    const int inst = blockIdx.x;
+    InstState& st = b.state[inst];
+    if (st.status != ST_RUNNING) return;
+    const InstPlan ip = b.insts[inst];
+    const DictPlan dp = b.dicts[ip.dict];
+    const unsigned best = (unsigned)(st.best32 >> 32);
+    if (best == 0u) {  // nothing beats 0: src/gabor.cpp:108-110
+        if (threadIdx.x == 0) {
+            st.status = ST_ERROR;
+            st.err = ERR_MAP_EMPTY;
+        }
+        return;
+    }
+    const unsigned thr = __float_as_uint(__uint_as_float(best) * (1.0f - b.band));
+    if (threadIdx.x == 0) st.nbins = 0;
+    for (int c = 0; c < dp.chunks; ++c) {
+        const unsigned long long ck = b.chunks[ip.chunk_off + c];
+        if ((unsigned)(ck >> 32) < thr) continue;
+        const long long s0 = (long long)c * kChunk;
+        const long long s1 = min(s0 + kChunk, dp.slots);
+        for (long long s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+            const unsigned long long v = b.slots[ip.slot_off + s];
+            if ((unsigned)(v >> 32) >= thr) {
+                const int at = atomicAdd(b.ctr + CTR_CSLOTS, 1);
+                if (at < b.cslot_cap) {
+                    CandSlot cs;
+                    cs.inst = inst;
+                    slot_to_jtg(b, dp, s, cs.j, cs.t, cs.g);
+                    b.cslots[at] = cs;
+                } else {
+                    st.err = ERR_CAND_OVERFLOW;
+                }
+            }
+        }
+    }
+}
+
+// FP64 value of one candidate bin and channel by direct DFT over its window
+// (GaborWorkspaceMap::compute, src/gabor.cpp:279-299, in FP64).
+__global__ void k_rescore(BatchDev b) {
+    __shared__ double2 red[32];
+    __shared__ int s_item;
+    const int nb = min(b.ctr[CTR_CBINS], b.cbin_cap);
+    const int total = nb * b.cmax;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(b.ctr + CTR_RESCORE_Q, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= total) break;
+        const int bin = item / b.cmax, c = item - bin * b.cmax;
+        const CandBin cb = b.cbins[bin];
+        const InstPlan ip = b.insts[cb.inst];
+        if (c >= ip.C) continue;
+        const DictPlan dp = b.dicts[ip.dict];
+        const ScalePlan sp = b.scales[dp.scale0 + cb.j];
+        const double fs = dp.fs;
+        const double t0 = grid_t(cb.t, dp.tMax, sp.tcount);
+        int iL, iR;
+        double t0fixed;
+        window_bounds(t0, sp.hw, fs, dp.N, iL, iR, t0fixed);
+        const int W = iR - iL + 1;
+        // gaussize, src/gabor.cpp:31-40
+        const double wg = sqrt(CUDART_PI) / sp.s;
+        const double ga = wg * (1.0 / fs);
+        const double gb = wg * t0fixed;
+        const double* x = b.residual + ip.res_off + (long long)c * dp.N + iL;
+        const long long nfft = sp.nfft;
+        const int T = blockDim.x;
+        const int chunk = (W + T - 1) / T;
+        const int n0 = threadIdx.x * chunk, n1 = min(W, n0 + chunk);
+        double sr = 0.0, si = 0.0;
+        if (n0 < n1) {
+            double ws, wc, ss, sc;
+            sincospi(-2.0 * (double)(((long long)cb.k * n0) & (nfft - 1)) / (double)nfft, &ws, &wc);
+            sincospi(-2.0 * (double)cb.k / (double)nfft, &ss, &sc);
+            for (int n = n0; n < n1; ++n) {
+                const double xw = __dsub_rn(__dmul_rn(ga, (double)n), gb);
+                const double v = x[n] * exp(-xw * xw);
+                sr += v * wc;
+                si += v * ws;
+                const double nc = wc * sc - ws * ss;
+                ws = wc * ss + ws * sc;
+                wc = nc;
+            }
+        }
+#pragma unroll
+        for (int off = 16; off; off >>= 1) {
+            sr += __shfl_down_sync(0xffffffffu, sr, off);
+            si += __shfl_down_sync(0xffffffffu, si, off);
+        }
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = make_double2(sr, si);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tr = 0.0, tim = 0.0;
+            for (int w = 0; w < (T >> 5); ++w) {
+                tr += red[w].x;
+                tim += red[w].y;
+            }
+            // value = (1/fs) X polar(1, f * 2 pi t0fixed), src/gabor.cpp:295-299
+            const double norm = 1.0 / fs;
+            const double f = (double)cb.k * fs / (double)nfft;
+            const double ang = f * (2 * CUDART_PI * t0fixed);
+            double sa, ca;
+            sincos(ang, &sa, &ca);
+            const double xr = norm * tr, xi = norm * tim;
+            b.cbin_v[(long long)bin * b.cmax + c] = make_double2(xr * ca - xi * sa, xr * sa + xi * ca);
+        }
+        __syncthreads();
+    }
+}
+
+// GaborComputer for one bin in FP64 (src/gabor.cpp:44-71), constraint first
+// for MMP1 at low frequency (src/mmp.cpp:9-21).  v is modified in place.
+struct Computer64 {
+    double normComplex, freqNyquist, f, f4Norm, expFactor, t;
+    bool isHighFreq;
+};
+
+__device__ __forceinline__ Computer64 make_computer64(const ScalePlan& sp, const DictPlan& dp, int k, int ti) {
+    Computer64 q;
+    q.normComplex = sqrt(1.41421356237309504880 / sp.s);
+    q.freqNyquist = 0.5 * dp.fs;
+    q.f = (double)k * dp.fs / (double)sp.nfft;
+    q.isHighFreq = q.f > 0.5 * q.freqNyquist;
+    q.f4Norm = q.isHighFreq ? (q.freqNyquist - q.f) : q.f;
+    q.expFactor = exp(-2 * CUDART_PI * sp.s * sp.s * q.f4Norm * q.f4Norm);
+    q.t = grid_t(ti, dp.tMax, sp.tcount);
+    return q;
+}
+
+__device__ __forceinline__ void mmp1_constraint64(double2* v, int C) {
+    double dr = 0.0, di = 0.0;
+    for (int c = 0; c < C; ++c) {
+        dr += v[c].x * v[c].x - v[c].y * v[c].y;
+        di += 2.0 * v[c].x * v[c].y;
+    }
+    const double angle = 0.5 * atan2(di, dr);
+    double sa, ca;
+    sincos(angle, &sa, &ca);
+    for (int c = 0; c < C; ++c) {
+        const double rho = hypot(v[c].x, v[c].y) * cos(atan2(v[c].y, v[c].x) - angle);
+        v[c] = make_double2(rho * ca, rho * sa);
+    }
+}
+
+__device__ __forceinline__ double norm_real(const Computer64& q, double phase) {
+    const double p4 = q.isHighFreq ? (2 * CUDART_PI * q.freqNyquist * q.t - phase) : phase;
+    return 1.41421356237309504880 * q.normComplex / sqrt(1.0 + cos(2 * p4) * q.expFactor);
+}
+
+constexpr int kMaxChannels = 64;
+
+// One CTA per instance: FP64 energies of its candidate bins, argmax (ties to
+// the lowest (scale, t, f)), atom parameters (src/gabor.cpp:111-131).
+__global__ void k_select(BatchDev b) {
+    __shared__ double s_e[128];
+    __shared__ unsigned long long s_key[128];
+    __shared__ int s_bin[128];
+    __shared__ double2 s_v[kMaxChannels];
+    const int inst = blockIdx.x;
+    InstState& st = b.state[inst];
+    if (st.status != ST_RUNNING) return;
+    const InstPlan ip = b.insts[inst];
+    const DictPlan dp = b.dicts[ip.dict];
+    const int C = ip.C;
+    const int nbins = min(st.nbins, b.inst_bin_cap);
+    if (st.err == ERR_CAND_OVERFLOW || nbins == 0) {
+        if (threadIdx.x == 0) {
+            st.status = ST_ERROR;
+            if (st.err == ERR_NONE) st.err = ERR_MAP_EMPTY;
+        }
+        return;
+    }
+    double be = -1.0;
+    unsigned long long bk = ~0ull;
+    int bbin = -1;
+    double2 v[kMaxChannels];
+    for (int i = threadIdx.x; i < nbins; i += blockDim.x) {
+        const int bin = b.inst_bins[(long long)inst * b.inst_bin_cap + i];
+        const CandBin cb = b.cbins[bin];
+        const ScalePlan sp = b.scales[dp.scale0 + cb.j];
+        const Computer64 q = make_computer64(sp, dp, cb.k, cb.t);
+        for (int c = 0; c < C; ++c) v[c] = b.cbin_v[(long long)bin * b.cmax + c];
+        if (b.mode == MODE_MMP1 && !q.isHighFreq) mmp1_constraint64(v, C);
+        double square = 0.0;
+        for (int c = 0; c < C; ++c) {
+            const double phase = atan2(v[c].y, v[c].x);
+            const double nr = norm_real(q, phase);
+            const double mod = hypot(v[c].x, v[c].y) * nr * sqrt(dp.fs);
+            square += mod * mod;
+        }
+        b.cbins[bin].e64 = square;
+        const unsigned long long key =
+            ((unsigned long long)cb.j << 48) | ((unsigned long long)cb.t << 20) | (unsigned long long)cb.k;
+        if (square > be || (square == be && key < bk)) {
+            be = square;
+            bk = key;
+            bbin = bin;
+        }
+    }
+    s_e[threadIdx.x] = be;
+    s_key[threadIdx.x] = bk;
+    s_bin[threadIdx.x] = bbin;
+    __syncthreads();
+    for (int off = blockDim.x / 2; off; off >>= 1) {
+        if (threadIdx.x < off) {
+            const double oe = s_e[threadIdx.x + off];
+            const unsigned long long ok = s_key[threadIdx.x + off];
+            if (oe > s_e[threadIdx.x] || (oe == s_e[threadIdx.x] && ok < s_key[threadIdx.x])) {
+                s_e[threadIdx.x] = oe;
+                s_key[threadIdx.x] = ok;
+                s_bin[threadIdx.x] = s_bin[threadIdx.x + off];
+            }
+        }
+        __syncthreads();
+    }
+    const int win = s_bin[0];
+    const CandBin cb = b.cbins[win];
+    const ScalePlan sp = b.scales[dp.scale0 + cb.j];
+    const Computer64 q = make_computer64(sp, dp, cb.k, cb.t);
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < C; ++c) s_v[c] = b.cbin_v[(long long)win * b.cmax + c];
+        if (b.mode == MODE_MMP1 && !q.isHighFreq) mmp1_constraint64(s_v, C);
+    }
+    __syncthreads();
+    const int it = st.it;
+    for (int c = threadIdx.x; c < C; c += blockDim.x) {
+        const double2 vc = s_v[c];
+        const double phase = atan2(vc.y, vc.x);
+        const double nr = norm_real(q, phase);
+        const double mag = hypot(vc.x, vc.y);
+        double* p = b.atoms + ip.out_off + ((long long)it * C + c) * 6;
+        p[0] = mag * nr * sqrt(dp.fs);
+        p[1] = mag * nr * nr;
+        p[2] = q.t * dp.fs;
+        p[3] = sp.s * dp.fs;
+        p[4] = q.f * 2.0 / dp.fs;
+        p[5] = phase;
+    }
+    if (threadIdx.x == 0) {
+        b.indices[(long long)inst * b.iter_max + it] = make_int4(cb.j, cb.t, cb.k, nbins);
+        st.it = it + 1;
+        if (st.it >= b.iter_max) st.status = ST_DONE;  // src/classes.cpp:57-59
+        atomicAdd(b.ctr + CTR_STAT_BINS, nbins);
+    }
+}
+
+// ------------------------------------------------------------ residual
+
+__device__ __forceinline__ double block_sum(double v, double* red) {
+#pragma unroll
+    for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0) {
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        red[32] = t;
+    }
+    __syncthreads();
+    t = red[32];
+    __syncthreads();
+    return t;
+}
+
+// Gabor waveform sample i of an atom window, subtractAtomFromSignal
+// (src/gabor.cpp:143-163).
+struct AtomWindow {
+    double sA, fA, tA, amplitude, omega, phase, ga, gb;
+    int iL, iR;
+};
+
+__device__ __forceinline__ AtomWindow atom_window(const double* params, double fs, int N, bool fit) {
+    AtomWindow a;
+    a.sA = params[3] / fs;
+    a.fA = params[4] * fs / 2.0;
+    a.tA = params[2] / fs;
+    a.amplitude = fit ? 1.0 : params[1];
+    a.omega = 2.0 * CUDART_PI * a.fA;
+    a.phase = params[5];
+    const double hw = 3.0 * a.sA;
+    long long l = __double2ll_rn(__dmul_rn(__dsub_rn(a.tA, hw), fs));
+    long long r = __double2ll_rn(__dmul_rn(__dadd_rn(a.tA, hw), fs));
+    a.iL = (int)(l > 0 ? l : 0);
+    a.iR = (int)(r < (long long)N - 1 ? r : (long long)N - 1);
+    const double wg = sqrt(CUDART_PI) / a.sA;
+    a.ga = wg * (1.0 / fs);
+    a.gb = wg * __dsub_rn(a.tA, __ddiv_rn((double)a.iL, fs));
+    return a;
+}
+
+__device__ __forceinline__ double atom_sample(const AtomWindow& a, int i, double fs) {
+    const double t = __dsub_rn(__ddiv_rn((double)(i + a.iL), fs), a.tA);
+    const double w = a.amplitude * cos(__dadd_rn(__dmul_rn(a.omega, t), a.phase));
+    const double xw = __dsub_rn(__dmul_rn(a.ga, (double)i), a.gb);
+    return w * exp(-xw * xw);
+}
+
+// One CTA per (instance, channel): residual -= atom (fit = false), then the
+// channel's energy sum(x^2)/fs (SingleSignal::computeEnergy, inc/base.hpp:39-46).
+__global__ void k_subtract(BatchDev b) {
+    __shared__ double red[33];
+    const int2 ic = b.blk_ic[blockIdx.x];
+    const int inst = ic.x, c = ic.y;
+    const InstState& st = b.state[inst];
+    if (st.status != ST_RUNNING) return;
+    const InstPlan ip = b.insts[inst];
+    const DictPlan dp = b.dicts[ip.dict];
+    const double fs = dp.fs;
+    double* x = b.residual + ip.res_off + (long long)c * dp.N;
+    const double* p = b.atoms + ip.out_off + ((long long)(st.it - 1) * ip.C + c) * 6;
+    const AtomWindow a = atom_window(p, fs, dp.N, false);
+    const int Nw = a.iR - a.iL + 1;
+    for (int i = threadIdx.x; i < Nw; i += blockDim.x) x[a.iL + i] -= atom_sample(a, i, fs);
+    __syncthreads();
+    double s = 0.0;
+    for (int i = threadIdx.x; i < dp.N; i += blockDim.x) s += x[i] * x[i];
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) b.chan_energy[ip.cen_off + c] = s / fs;
+}
+
+// One CTA per (instance, channel): residual from the float32 input
+// (src/io.cpp:33 converts to double; MMP2 sums channels, src/mmp.cpp:24-32)
+// unless the caller wrote the residual itself, its energy, and the instance
+// state.
+__global__ void k_init(BatchDev b, int from_input) {
+    __shared__ double red[33];
+    const int2 ic = b.blk_ic[blockIdx.x];
+    const int inst = ic.x, c = ic.y;
+    const InstPlan ip = b.insts[inst];
+    const DictPlan dp = b.dicts[ip.dict];
+    const float* in = b.input + ip.in_off;
+    const int Cin = ip.in_channels;
+    double* x = b.residual + ip.res_off + (long long)c * dp.N;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < dp.N; i += blockDim.x) {
+        double v;
+        if (!from_input) {
+            v = x[i];
+        } else if (ip.chan0 == -2) {
+            v = (double)in[(long long)i * Cin];
+            for (int k = 1; k < Cin; ++k) v += (double)in[(long long)i * Cin + k];
+        } else if (ip.chan0 >= 0) {
+            v = (double)in[(long long)i * Cin + ip.chan0];
+        } else {
+            v = (double)in[(long long)i * Cin + c];
+        }
+        if (from_input) x[i] = v;
+        s += v * v;
+    }
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) {
+        b.chan_energy[ip.cen_off + c] = s / dp.fs;
+        if (c == 0) {
+            InstState& st = b.state[inst];
+            st.status = ST_RUNNING;
+            st.it = 0;
+            st.err = ERR_NONE;
+            st.nbins = 0;
+            st.best32 = 0;
+        }
+    }
+}
+
+// Workspace::subtractAtomFromSignal on one FP64 signal (src/gabor.cpp:143-187),
+// fit or not; a single CTA.  params (6) are updated in place when fitting.
+__global__ void k_subtract_signal(double* x, int N, double fs, double* params, int fit) {
+    __shared__ double red[33];
+    double p[6];
+    for (int k = 0; k < 6; ++k) p[k] = params[k];
+    const AtomWindow w = atom_window(p, fs, N, fit != 0);
+    const int Nw = w.iR - w.iL + 1;
+    if (Nw <= 0) return;
+    double norm = 1.0, dot = 1.0;
+    if (fit) {
+        double n2 = 0.0, d = 0.0;
+        for (int i = threadIdx.x; i < Nw; i += blockDim.x) {
+            const double v = atom_sample(w, i, fs);
+            n2 += v * v;
+        }
+        n2 = block_sum(n2, red);
+        norm = sqrt(n2);
+        for (int i = threadIdx.x; i < Nw; i += blockDim.x) d += (atom_sample(w, i, fs) / norm) * x[w.iL + i];
+        dot = block_sum(d, red);
+    }
+    for (int i = threadIdx.x; i < Nw; i += blockDim.x) {
+        const double v = atom_sample(w, i, fs);
+        x[w.iL + i] -= fit ? (v / norm) * dot : v;
+    }
+    if (fit && threadIdx.x == 0) {
+        params[0] = dot;
+        params[1] = dot / norm;
+    }
+}
+
+// MMP2 per-channel fit (src/mmp.cpp:36-43 with subtractAtomFromSignal's fit
+// branch, src/gabor.cpp:165-183): one CTA per (epoch, channel), atoms in
+// order, each projected on the channel's residual in FP64.
+__global__ void k_mmp2_fit(BatchDev b, const int2* fit_map, double* fit_atoms, int fit_cap) {
+    __shared__ double red[33];
+    const int2 ec = fit_map[blockIdx.x];  // (instance of the channel sum, input channel)
+    const int inst = ec.x, c = ec.y;
+    const InstPlan ip = b.insts[inst];
+    const DictPlan dp = b.dicts[ip.dict];
+    const InstState& st = b.state[inst];
+    const double fs = dp.fs;
+    const float* in = b.input + ip.in_off;
+    const int Cin = ip.in_channels;
+    extern __shared__ double xs[];
+    for (int i = threadIdx.x; i < dp.N; i += blockDim.x) xs[i] = (double)in[(long long)i * Cin + c];
+    __syncthreads();
+    const int n = min(st.it, fit_cap);
+    for (int a = 0; a < n; ++a) {
+        const double* p0 = b.atoms + ip.out_off + (long long)a * 6;
+        double* po = fit_atoms + ((long long)blockIdx.x * fit_cap + a) * 6;
+        double p[6];
+        for (int k = 0; k < 6; ++k) p[k] = p0[k];
+        const AtomWindow w = atom_window(p, fs, dp.N, true);
+        const int Nw = w.iR - w.iL + 1;
+        double n2 = 0.0, dot = 0.0;
+        for (int i = threadIdx.x; i < Nw; i += blockDim.x) {
+            const double v = atom_sample(w, i, fs);
+            n2 += v * v;
+        }
+        n2 = block_sum(n2, red);
+        const double norm = sqrt(n2);
+        for (int i = threadIdx.x; i < Nw; i += blockDim.x) {
+            const double v = atom_sample(w, i, fs) / norm;
+            dot += v * xs[w.iL + i];
+        }
+        dot = block_sum(dot, red);
+        for (int i = threadIdx.x; i < Nw; i += blockDim.x) {
+            const double v = atom_sample(w, i, fs) / norm;
+            xs[w.iL + i] -= v * dot;
+        }
+        if (threadIdx.x == 0) {
+            po[0] = dot;
+            po[1] = dot / norm;
+            for (int k = 2; k < 6; ++k) po[k] = p[k];
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace empi

@@ -1,0 +1,218 @@
+/*
+ * empi_b200 -- C ABI of the B200 Matching Pursuit engine.
+ *
+ * Plain C types only: pointers, sizes, doubles.  Every call is synchronous
+ * with respect to the caller's buffers (host data is copied before return);
+ * device work runs on the engine's stream.  One engine per host thread, or
+ * external locking.  Errors return an empi_status and leave a camelCase
+ * message (the reference's exception texts where one exists) readable with
+ * empi_last_error().
+ *
+ * Reference interfaces replaced (paths in the empi project):
+ *   empi_workspace_*      Workspace / WorkspaceBuilder seam, inc/classes.hpp:63-80,
+ *                         implemented there by GaborWorkspace (src/gabor.cpp:75-252)
+ *   empi_subtract_atom_from_signal
+ *                         Workspace::subtractAtomFromSignal, src/classes.cpp:15-22,
+ *                         src/gabor.cpp:143-187
+ *   empi_batch_*          Decomposition::compute and its SMP/MMP1/MMP2/MMP3
+ *                         overrides (src/classes.cpp:26-87, src/mmp.cpp:9-45,
+ *                         inc/mmp.hpp:11-31), run for many epochs at once
+ *   empi_run_config       the empi CLI body, src/empi.cpp:49-167 (config file in,
+ *                         SVAROG book out, stdout progress protocol)
+ *   empi_book_write       BookWriter::write, src/io.cpp:104-168
+ */
+#ifndef EMPI_B200_H
+#define EMPI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EMPI_B200_ABI_VERSION 1
+
+typedef enum {
+    EMPI_OK = 0,
+    EMPI_ERR_INVALID_ARGUMENT = 1,
+    EMPI_ERR_CUDA = 2,
+    EMPI_ERR_OUT_OF_MEMORY = 3,        /* insufficientMemory */
+    EMPI_ERR_SIGNAL_IS_EMPTY = 4,      /* signalIsEmpty (src/classes.cpp:35-39) */
+    EMPI_ERR_ENERGY_MAP_IS_EMPTY = 5,  /* energyMapIsEmpty (src/gabor.cpp:108-110) */
+    EMPI_ERR_SIGNAL_TOO_LONG = 6,      /* signalFileIsTooLongForThisDecomposition */
+    EMPI_ERR_CANDIDATE_OVERFLOW = 7,   /* more near-tied candidates than the engine holds */
+    EMPI_ERR_CONFIG = 8,               /* configuration errors (src/empi.cpp:59-141) */
+    EMPI_ERR_IO = 9,                   /* file errors (src/io.cpp) */
+    EMPI_ERR_NO_DEVICE = 10,
+    EMPI_ERR_INTERNAL = 11
+} empi_status;
+
+/* MP variants, src/empi.cpp:114-130 */
+typedef enum { EMPI_SMP = 0, EMPI_MMP1 = 1, EMPI_MMP2 = 2, EMPI_MMP3 = 3 } empi_variant;
+
+typedef struct empi_engine empi_engine;
+typedef struct empi_workspace empi_workspace;
+typedef struct empi_batch empi_batch;
+
+/* Thread-local message of the last failed call ("" after success). */
+const char* empi_last_error(void);
+const char* empi_status_string(empi_status status);
+int empi_abi_version(void);
+
+/* ---------------------------------------------------------------- engine */
+
+typedef struct {
+    int device;              /* CUDA ordinal */
+    void* stream;            /* cudaStream_t to run on; NULL = engine-owned stream */
+    int transform_cap;       /* largest shared-memory sub-FFT (16..4096, power of 2); 0 = default */
+    double candidate_band;   /* relative FP32 band re-scored in FP64; 0 = default (1e-4) */
+    int candidate_capacity;  /* candidate bins per iteration over a batch; 0 = default */
+    int iterations_per_graph;/* MP iterations per CUDA-graph launch; 0 = default */
+    int timing;              /* nonzero: record CUDA events around every refresh launch */
+} empi_engine_opts;
+
+void empi_engine_opts_default(empi_engine_opts* opts);
+empi_status empi_engine_create(const empi_engine_opts* opts, empi_engine** out);
+void empi_engine_destroy(empi_engine* engine);
+
+/* GaborWorkspaceBuilder(energyError, scaleMin, scaleMax, freqMax), src/gabor.cpp:213 */
+typedef struct {
+    double energy_error;
+    double scale_min;   /* seconds; 0 = default (2 samples) */
+    double scale_max;   /* seconds; INFINITY = default (signal length) */
+    double freq_max;    /* hertz; INFINITY = no limit */
+} empi_dictionary;
+
+/* Dictionary size (sum of fCount * tCount, GaborWorkspace::getAtomCount,
+ * src/gabor.cpp:135-141) and scale count for a signal shape. */
+empi_status empi_dictionary_size(const empi_dictionary* dict, double fs, int samples,
+                                 uint64_t* atom_count, int* scale_count);
+
+/* Scale table of a dictionary: s (seconds), Nfft, fCount, tCount per scale,
+ * as the reference's prepareWorkspace builds them.  Arrays hold cap entries. */
+empi_status empi_dictionary_scales(const empi_dictionary* dict, double fs, int samples, int cap,
+                                   double* s, int* nfft, int* fcount, int* tcount, int* count);
+
+/* -------------------------------------------------- workspace (the seam) */
+
+/* WorkspaceBuilder::prepareWorkspace(fs, channelCount, sampleCount, constraint),
+ * inc/classes.hpp:76-80.  `variant` selects the constraint: EMPI_MMP1 applies
+ * Mmp1Decomposition::constraint (src/mmp.cpp:9-21), the others none. */
+empi_status empi_workspace_create(empi_engine* engine, const empi_dictionary* dict, double fs,
+                                  int channels, int samples, empi_variant variant,
+                                  empi_workspace** out);
+void empi_workspace_destroy(empi_workspace* ws);
+
+/* Workspace::compute(const MultiSignal&): samples are channel-major,
+ * channels x samples doubles. */
+empi_status empi_workspace_compute(empi_workspace* ws, const double* samples);
+
+/* Workspace::findBestMatch(): writes channels x 6 params (modulus, amplitude,
+ * t*fs, s*fs, f*2/fs, phase) as src/gabor.cpp:111-131; index (optional) gets
+ * the winner's (scale, t, f) indices. */
+empi_status empi_workspace_find_best(empi_workspace* ws, double* params, int* index);
+
+/* Workspace::getAtomCount() */
+empi_status empi_workspace_atom_count(const empi_workspace* ws, uint64_t* count);
+
+/* Workspace::subtractAtom(atom, signal, channel): subtracts the atom from
+ * `samples` (one channel, in/out, `samples` doubles long) and refreshes the
+ * affected part of that channel's maps. */
+empi_status empi_workspace_subtract_atom(empi_workspace* ws, const double* params,
+                                         double* samples, int channel);
+
+/* Energy maps of one scale for parity checks: energy [f][t] (fCount x tCount
+ * floats, the FP32 values the engine ranks) -- optional, may be NULL. */
+empi_status empi_workspace_energy_map(empi_workspace* ws, int scale, float* energy);
+
+/* Workspace::subtractAtomFromSignal(atom, signal, fit): params (6, in/out when
+ * fit), samples (in/out, n doubles). Runs on the engine's device. */
+empi_status empi_subtract_atom_from_signal(empi_engine* engine, double* params, double* samples,
+                                           int n, double fs, int fit);
+
+/* ------------------------------------------------ batched decomposition */
+
+/* DecompositionSettings, inc/classes.hpp:84-87 */
+typedef struct {
+    int iteration_max;
+    double residual_energy;  /* stop when residue/total <= this; 1 - energyPercent/100 */
+} empi_settings;
+
+/* One epoch: samples x channels float32, sample-major (channels interleaved),
+ * the layout of empi's input files (src/io.cpp:28-34). */
+typedef struct {
+    double fs;
+    int channels;
+    int samples;
+    const float* data;
+} empi_epoch;
+
+/* Allocates device state for `count` epochs of the given shapes (data
+ * pointers are not read).  All epochs use `variant`; each epoch's dictionary
+ * follows its own fs and length. */
+empi_status empi_batch_create(empi_engine* engine, empi_variant variant, const empi_dictionary* dict,
+                              const empi_settings* settings, const empi_epoch* epochs, int count,
+                              empi_batch** out);
+void empi_batch_destroy(empi_batch* batch);
+
+/* Copies each epoch's host data to the device (shapes must match). */
+empi_status empi_batch_load(empi_batch* batch, const empi_epoch* epochs);
+
+/* Runs the decomposition of all loaded epochs to completion. */
+empi_status empi_batch_run(empi_batch* batch);
+
+/* Atoms of one epoch: atoms[c][a][6] for c < channels, a < cap (same params
+ * as find_best; MMP2 per-channel fits as src/mmp.cpp:36-43); count receives
+ * the atom count per channel.  energies (optional): residual energy after
+ * each iteration of the loop that produced the channel's atoms
+ * ([channel][cap] for SMP, [cap] otherwise; NaN where none was computed).
+ * indices (optional): (scale, t, f) per atom, same layout as energies x 3. */
+empi_status empi_batch_atoms(empi_batch* batch, int epoch, int cap, double* atoms, int* count,
+                             double* energies, int* indices);
+
+/* Total energy (src/classes.cpp:35, sum x^2 / fs) of each MP loop of an
+ * epoch: one per channel for SMP, one otherwise (the channel sum for MMP2). */
+empi_status empi_batch_total_energy(empi_batch* batch, int epoch, double* totals);
+
+typedef struct {
+    int iterations;           /* MP iterations run (max over loops) */
+    int atoms;                /* atoms emitted over all loops */
+    long long refresh_units;  /* shared-memory FFT work units executed */
+    long long windows;        /* (window, group) slots recomputed */
+    double fft_flops;         /* reference-equivalent FFT flops executed: 2.5 Nfft log2 Nfft per window */
+    double algorithmic_bytes; /* compulsory HBM bytes of the refreshes: residual spans + slot writes */
+    double refresh_ms;        /* summed CUDA-event time of refresh launches (timing opt) */
+    int refresh_launches;
+    int kernel_launches;      /* kernels launched by the last run */
+    int candidate_bins;       /* FP64 re-scored bins over the last run */
+    double run_ms;            /* device time of the last empi_batch_run */
+} empi_batch_stats;
+
+empi_status empi_batch_get_stats(empi_batch* batch, empi_batch_stats* stats);
+
+/* One-shot convenience: create + load + run; atoms of epoch e go to
+ * atoms + e * channels_e * cap * 6 in order (counts likewise per channel). */
+empi_status empi_decompose(empi_engine* engine, empi_variant variant, const empi_dictionary* dict,
+                           const empi_settings* settings, const empi_epoch* epochs, int count,
+                           int cap, double* atoms, int* counts);
+
+/* ------------------------------------------------------ host surface */
+
+/* Runs a complete empi job from a config file (src/empi.cpp:49-167):
+ * reads the signal, decomposes on the GPU, writes the SVAROG book and
+ * prints the START/CHANNEL/ATOM/END protocol to stdout. */
+empi_status empi_run_config(const char* config_path, const empi_engine_opts* opts);
+
+/* BookWriter::write for one epoch (src/io.cpp:104-168); `header` nonzero
+ * writes the file header first (epoch 1).  samples: channels x n floats
+ * channel-major; atoms: [c][cap][6]; counts per channel. */
+empi_status empi_book_write(const char* path, int append, int epoch_number, double fs, int channels,
+                            int n, const float* samples, int cap, const double* atoms,
+                            const int* counts);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EMPI_B200_H */

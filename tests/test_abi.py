@@ -1,0 +1,97 @@
+"""The C ABI library without a GPU: it loads, exports every symbol the header
+declares, and its host-side parts (dictionary geometry, config parsing, book
+writing) match the reference."""
+import math
+import os
+import re
+
+import numpy as np
+import pytest
+
+import empi_b200
+from helpers import GOLDEN, case_signal, golden
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    text = open(os.path.join(ROOT, "include", "empi_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(empi_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_function():
+    L = empi_b200.load_library()
+    names = header_functions()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(names) == set(empi_b200.EXPORTS)
+    assert L.empi_abi_version() == 1
+
+
+@pytest.mark.parametrize("fs,n,eps", [(128.0, 1280, 0.01), (256.0, 5120, 0.01), (512.0, 16384, 0.005),
+                                      (512.0, 16384, 0.001), (256.0, 513, 0.01)])
+def test_dictionary_matches_oracle(fs, n, eps):
+    got = empi_b200.dictionary_scales(eps, fs, n)
+    ref = O.geometry(fs, n, eps)
+    assert len(got) == len(ref)
+    for a, b in zip(got, ref):
+        assert a[1:] == b[1:]
+        assert a[0] == b[0]
+
+
+def test_dictionary_with_limits():
+    got = empi_b200.dictionary_scales(0.01, 100.0, 1000, 0.05, 3.0, 30.0)
+    assert got == [tuple(v) for v in O.geometry(100.0, 1000, 0.01, 0.05, 3.0, 30.0)]
+
+
+def test_book_writer_is_byte_identical_to_reference(tmp_path):
+    case = [c for c in golden()["cases"] if c["name"] == "smp0"][0]
+    fs, x = case_signal(case)
+    atoms = np.array(case["atoms"])  # [1, n, 6]
+    path = tmp_path / "book.b"
+    empi_b200.book_write(path, 1, fs, x.T, atoms, case["counts"])
+    assert path.read_bytes() == open(os.path.join(GOLDEN, "smp0.b"), "rb").read()
+
+
+def write_cfg(d, **kv):
+    base = dict(energyError="0.01", maximalNumberOfIterations="5", energyPercent="99.0", MP="SMP",
+                nameOfDataFile=str(d / "sig.bin"), nameOfOutputDirectory=str(d), samplingFrequency="128.0",
+                numberOfChannels="2", selectedChannels="1-2")
+    base.update(kv)
+    p = d / "cfg"
+    p.write_text("# comment line\n" + "".join(f"{k} {v}\n" for k, v in base.items() if v is not None))
+    return p
+
+
+@pytest.mark.parametrize("kv,msg", [
+    (dict(energyError=None), "missingConfigurationEntry:energyError"),
+    (dict(energyError="1.5"), "invalidEnergyErrorValue"),
+    (dict(maximalNumberOfIterations="0"), "invalidMaximalNumberOfIterations"),
+    (dict(energyPercent="100.5"), "invalidEnergyPercentValue"),
+    (dict(nameOfDataFile="/nonexistent/sig.bin"), "couldNotOpenSignalFile"),
+    (dict(samplingFrequency="0"), "invalidSamplingFrequency"),
+    (dict(numberOfChannels="-1"), "invalidNumberOfChannels"),
+    (dict(selectedChannels="1-3"), "invalidSubsetSpecification"),
+    (dict(MP="XYZ"), "unsupportedDecompositionType"),
+    (dict(numberOfSamplesInEpoch="0"), "invalidNumberOfSamplesInEpoch"),
+    (dict(selectedEpochs="1"), "missingConfigurationEntry:numberOfSamplesInEpoch"),
+])
+def test_config_errors_match_reference_messages(tmp_path, kv, msg):
+    np.zeros(256, np.float32).tofile(tmp_path / "sig.bin")
+    cfg = write_cfg(tmp_path, **kv)
+    with pytest.raises(empi_b200.EmpiError) as ei:
+        empi_b200.run_config(cfg)
+    assert ei.value.message == msg
+
+
+def test_synth_workloads_are_seeded():
+    from empi_b200 import synth
+
+    a = synth.workload(1, epochs=1, channels=2, samples=300)
+    b = synth.workload(1, epochs=1, channels=2, samples=300)
+    assert np.array_equal(a.epochs[0], b.epochs[0])
+    w = synth.workload(3, epochs=5)
+    assert len(w.epochs) == 5 and all(512 <= e.shape[0] <= 16384 for e in w.epochs)

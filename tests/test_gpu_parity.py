@@ -1,0 +1,215 @@
+"""Parity of the sm_100a engine with the oracle and the reference goldens.
+
+Tolerances: FP32 energy maps within 2e-6 of the map maximum and 2e-5
+relative on entries above 1% of it; atom sequences by the rule in
+helpers.py (indices exact unless the oracle margin is < 1e-6; amplitude 1e-5
+relative; phase 1e-5 rad; residual energy 1e-6 relative)."""
+import math
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import empi_b200
+from helpers import GOLDEN, case_limits, case_signal, compare_sequences, golden
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+CASES = golden()["cases"]
+
+
+def workload0():
+    from empi_b200 import synth
+
+    w = synth.workload(0)
+    return w.fs, w.epochs[0].T.astype(np.float64)
+
+
+@pytest.mark.parametrize("scale", [0, 1, 4, 12, 20, 27, 33])
+def test_energy_map_fp32_matches_fp64_oracle(engine, scale):
+    fs, x = workload0()
+    ws = empi_b200.GaborWorkspaceBuilder(0.01, engine=engine).prepareWorkspace(fs, 1, x.shape[1])
+    ws.compute(x)
+    got = ws.energy_map(scale).astype(np.float64)
+    ref = O.energy_map(fs, x, 0.01, scale)
+    assert got.shape == ref.shape
+    top = ref.max()
+    assert np.max(np.abs(got - ref)) <= 2e-6 * top
+    big = ref > 1e-2 * top
+    assert np.max(np.abs(got[big] - ref[big]) / ref[big]) <= 2e-5
+    ws.close()
+
+
+@pytest.mark.parametrize("variant,mmp1", [("mmp3", False), ("mmp1", True)])
+def test_multichannel_energy_maps(engine, variant, mmp1):
+    from empi_b200 import synth
+
+    w = synth.workload(1, epochs=1, channels=4, samples=900, seed=3)
+    x = w.epochs[0].T.astype(np.float64)
+    ws = empi_b200.GaborWorkspaceBuilder(0.01, engine=engine).prepareWorkspace(
+        w.fs, 4, 900, constraint=empi_b200.MMP1 if mmp1 else None)
+    ws.compute(x)
+    g = O.geometry(w.fs, 900, 0.01)
+    for j in (0, len(g) // 3, len(g) // 2, len(g) - 1):
+        got = ws.energy_map(j).astype(np.float64)
+        ref = O.energy_map(w.fs, x, 0.01, j, mmp1=mmp1)
+        top = ref.max()
+        assert np.max(np.abs(got - ref)) <= 3e-6 * top, (variant, j)
+    ws.close()
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_decomposition_matches_reference_golden(engine, case):
+    fs, x = case_signal(case)
+    lim = case_limits(case)
+    res = empi_b200.decompose_epochs(case["variant"], [x], fs, case["energy_error"], case["iterations"],
+                                     case["energy_percent"], lim["smin"], lim["smax"], lim["fmax"], engine)[0]
+    ora = O.decompose(case["variant"], fs, x.T.astype(np.float64), case["energy_error"], case["iterations"],
+                      case["energy_percent"], **lim)
+    smp = case["variant"] == "smp" or x.shape[1] == 1
+    for c in range(x.shape[1]):
+        ref = case["atoms"][c]
+        got = res.atoms[c, : res.counts[c]]
+        margins = ora.margins[c if smp else 0]
+        e_ref = case["energies"][c if smp else 0]
+        e_got = res.energies[c] if smp else res.energies
+        # MMP2 per-channel fits carry no loop energies of their own
+        compare_sequences(ref, got, margins, e_ref if case["variant"] != "mmp2" or c == 0 else None,
+                          e_got, label=f"{case['name']} ch{c}")
+
+
+def test_workspace_seam_step_by_step(engine):
+    case = [c for c in CASES if c["name"] == "mmp3_3ch_1024"][0]
+    fs, x = case_signal(case)
+    C, N = x.shape[1], x.shape[0]
+    sig = [np.ascontiguousarray(x[:, c].astype(np.float64)) for c in range(C)]
+    ws = empi_b200.GaborWorkspaceBuilder(case["energy_error"], engine=engine).prepareWorkspace(fs, C, N)
+    ws.compute(np.stack(sig))
+    ora = O.decompose("mmp3", fs, x.T.astype(np.float64), case["energy_error"], 6, 100.0)
+    for it in range(5):
+        atoms, idx = ws.findBestMatch(with_index=True)
+        if ora.margins[0][it] >= 1e-6:
+            assert tuple(idx) == tuple(ora.indices[0][it])
+        for c in range(C):
+            ref = case["atoms"][c][it]
+            np.testing.assert_allclose(atoms[c].params[:2], ref[:2], rtol=1e-5)
+            np.testing.assert_allclose(atoms[c].params[2:5], ref[2:5], rtol=1e-12)
+            before = sig[c].copy()
+            ws.subtractAtom(atoms[c], sig[c], c)
+            _, expect = O.subtract_atom(atoms[c].params, before, fs, False)
+            np.testing.assert_allclose(sig[c], expect, rtol=0, atol=1e-12 * np.max(np.abs(before)))
+    ws.close()
+
+
+def test_atom_count_matches_reference(engine):
+    ws = empi_b200.GaborWorkspaceBuilder(0.01, engine=engine).prepareWorkspace(128.0, 1, 1280)
+    assert ws.getAtomCount() == 5008073
+    ws.close()
+
+
+@pytest.mark.parametrize("fit", [False, True])
+def test_subtract_atom_from_signal(engine, fit):
+    rng = np.random.default_rng(4)
+    fs = 200.0
+    x = rng.standard_normal(1500)
+    params = [0.0, 2.5, 700.0, 0.8 * fs, 12.0 * 2 / fs, 0.7]
+    p_ref, y_ref = O.subtract_atom(params, x, fs, fit)
+    y = x.copy()
+    p = empi_b200.GaborWorkspace.subtractAtomFromSignal(list(params), y, fit, fs, engine)
+    np.testing.assert_allclose(y, y_ref, rtol=0, atol=1e-12)
+    if fit:
+        np.testing.assert_allclose(p[:2], p_ref[:2], rtol=1e-12)
+
+
+def test_uneven_batch_matches_oracle(engine):
+    from empi_b200 import synth
+
+    rng = np.random.default_rng(9)
+    epochs = []
+    for n, c in [(512, 1), (1000, 2), (777, 1), (2048, 3), (600, 2)]:
+        epochs.append(np.stack([synth.smp_channel(rng, n, 256.0, 6, 10.0) for _ in range(c)], 1).astype(np.float32))
+    settings = empi_b200.DecompositionSettings(12, 0.005)
+    b = empi_b200.Batch("smp", 0.01, settings, [e.shape for e in epochs], 256.0, engine=engine)
+    b.load(epochs)
+    b.run()
+    for e, ep in enumerate(epochs):
+        res = b.result(e)
+        ora = O.decompose("smp", 256.0, ep.T.astype(np.float64), 0.01, 12, 99.5)
+        for c in range(ep.shape[1]):
+            ref = ora.atoms[c, : ora.natoms[c]]
+            compare_sequences(ref, res.atoms[c, : res.counts[c]], ora.margins[c], ora.energies[c],
+                              res.energies[c], label=f"epoch {e} ch {c}")
+    b.close()
+
+
+def test_signal_is_empty(engine):
+    with pytest.raises(empi_b200.EmpiError) as ei:
+        empi_b200.decompose_epochs("smp", [np.zeros((256, 1), np.float32)], 128.0, 0.01, 5, 99.0, engine=engine)
+    assert ei.value.message == "signalIsEmpty"
+
+
+def test_batch_rerun_is_deterministic(engine):
+    from empi_b200 import synth
+
+    w = synth.workload(1, epochs=2, channels=3, samples=1024, seed=77)
+    settings = empi_b200.DecompositionSettings(15, 0.0)
+    b = empi_b200.Batch("mmp2", 0.01, settings, [e.shape for e in w.epochs], w.fs, engine=engine)
+    b.load(w.epochs)
+    b.run()
+    r1 = [b.result(e) for e in range(2)]
+    b.run()
+    r2 = [b.result(e) for e in range(2)]
+    for a, c in zip(r1, r2):
+        assert np.array_equal(a.atoms, c.atoms)
+        assert np.array_equal(a.counts, c.counts)
+    b.close()
+
+
+def decode_book(data):
+    """Minimal MPv5 decoder (field conversions of the reference's utils/readbook.cpp)."""
+    import struct
+
+    pos = 6
+    out = {"atoms": []}
+    while pos < len(data):
+        bid = data[pos]
+        ln = struct.unpack(">I", data[pos + 1:pos + 5])[0]
+        if bid in (1, 2):
+            pos += 5 + ln
+        elif bid == 7:
+            pos += 11
+        elif bid == 8:
+            pos += 5 + ln
+        elif bid == 9:
+            end = pos + 5 + ln
+            pos += 7
+            while pos < end:
+                vals = struct.unpack(">6f", data[pos + 2:pos + 26])
+                out["atoms"].append(vals)
+                pos += 26
+        else:
+            raise ValueError(bid)
+    return out
+
+
+def test_cli_book_matches_reference(tmp_path):
+    case = [c for c in CASES if c["name"] == "smp0"][0]
+    fs, x = case_signal(case)
+    x.astype(np.float32).tofile(tmp_path / "smp0.bin")
+    (tmp_path / "smp0.cfg").write_text(open(os.path.join(GOLDEN, "smp0.cfg")).read())
+    cli = os.path.join(os.path.dirname(empi_b200.LIB_PATH), "empi-gpu")
+    p = subprocess.run([cli, "-x", "smp0.cfg"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stdout + p.stderr
+    assert p.stdout.splitlines()[:3] == open(os.path.join(GOLDEN, "smp0.stdout")).read().splitlines()[:3]
+    assert p.stdout.rstrip().endswith("END")
+    got = (tmp_path / "smp0_smp.b").read_bytes()
+    ref = open(os.path.join(GOLDEN, "smp0.b"), "rb").read()
+    assert len(got) == len(ref)
+    head = 6 + 9 + 32 + 11 + 7 + 4 * 1280
+    assert got[:head] == ref[:head]
+    ga, ra = decode_book(got)["atoms"], decode_book(ref)["atoms"]
+    assert len(ga) == len(ra) == 50
+    for g, r in zip(ga, ra):
+        assert all(abs(a - b) <= 2e-5 * max(1.0, abs(b)) for a, b in zip(g[:5], r[:5]))
