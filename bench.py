@@ -43,6 +43,11 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    # small cases for profiling runs (not bench numbers)
+    p.add_argument("--epochs", type=int, default=0, help="decompose only the first E epochs")
+    p.add_argument("--iterations", type=int, default=0, help="override the iteration count")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-roofline", action="store_true")
     return p.parse_args()
 
 
@@ -224,7 +229,8 @@ def ours(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-    w = synth.workload(WORKLOAD, seed=1000 + WORKLOAD + 7919 * rank)
+    w = synth.workload(WORKLOAD, seed=1000 + WORKLOAD + 7919 * rank, epochs=args.epochs or None,
+                       iterations=args.iterations or None)
     stream = torch.cuda.Stream()
     eng = empi_b200.Engine(device=local, stream=stream.cuda_stream)
     settings = empi_b200.DecompositionSettings(w.iterations, 1.0 - 0.01 * w.energy_percent)
@@ -272,7 +278,7 @@ def ours(args):
     e2e_ms = 0.0
     d2h = 0
     barrier()
-    for _ in range(args.steps):
+    for _ in range(0 if args.no_e2e else args.steps):
         with torch.cuda.stream(stream):
             flush.fill_(1.0)
             e0 = torch.cuda.Event(enable_timing=True)
@@ -297,32 +303,34 @@ def ours(args):
     total_ms, e2e_ms = float(t[0]), float(t[1])
     units = atoms_per_step * args.steps * world
     value = units / (total_ms / 1e3)
-    e2e_value = units / (e2e_ms / 1e3)
+    e2e_value = units / (e2e_ms / 1e3) if e2e_ms > 0 else None
 
     # dominant kernel (k_refresh): CUDA events around every refresh launch
     eng_t = empi_b200.Engine(device=local, stream=stream.cuda_stream, timing=True)
     bt = empi_b200.Batch(w.variant, w.energy_error, settings, shapes, w.fs, engine=eng_t)
     bt.load(host)
-    bt.run()
-    bt.run()
+    for _ in range(0 if args.no_roofline else 2):
+        bt.run()
     st = bt.stats()
-    per_launch_ms = st.refresh_ms / max(1, st.refresh_launches)
-    bytes_per_launch = st.algorithmic_bytes / max(1, st.refresh_launches)
-    flops_per_launch = st.fft_flops / max(1, st.refresh_launches)
-    peaks, peak_kind = measured_peaks()
-    achieved_gbs = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
-    tr = profiled_traffic()
-    roofline = {"kernel": "k_refresh (windowed FFT + energy + slot max)", "bound": "hbm",
-                "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved_gbs / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs",
-                "traffic": tr.get("dram_bytes_per_launch") if tr else None,
-                "launch_ms": per_launch_ms, "launches": st.refresh_launches,
-                "algorithmic_bytes_per_launch": bytes_per_launch}
-    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
-    roofline_fp32 = {"achieved": flops_per_launch / (per_launch_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
-                     "peak": fp32_peak, "peak_source": "nominal FP32 CUDA-core (148 SMs x 128 x 2 x 1.965 GHz)",
-                     "frac": flops_per_launch / (per_launch_ms * 1e-3) / 1e12 / fp32_peak,
-                     "flops": "reference-equivalent 2.5 Nfft log2 Nfft per refreshed window"}
+    roofline = roofline_fp32 = None
+    if st.refresh_launches:
+        per_launch_ms = st.refresh_ms / max(1, st.refresh_launches)
+        bytes_per_launch = st.algorithmic_bytes / max(1, st.refresh_launches)
+        flops_per_launch = st.fft_flops / max(1, st.refresh_launches)
+        peaks, peak_kind = measured_peaks()
+        achieved_gbs = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
+        tr = profiled_traffic()
+        roofline = {"kernel": "k_refresh (windowed FFT + energy + slot max)", "bound": "hbm",
+                    "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": achieved_gbs / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs",
+                    "traffic": tr.get("dram_bytes_per_launch") if tr else None,
+                    "launch_ms": per_launch_ms, "launches": st.refresh_launches,
+                    "algorithmic_bytes_per_launch": bytes_per_launch}
+        fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
+        roofline_fp32 = {"achieved": flops_per_launch / (per_launch_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+                         "peak": fp32_peak, "peak_source": "nominal FP32 CUDA-core (148 SMs x 128 x 2 x 1.965 GHz)",
+                         "frac": flops_per_launch / (per_launch_ms * 1e-3) / 1e12 / fp32_peak,
+                         "flops": "reference-equivalent 2.5 Nfft log2 Nfft per refreshed window"}
     bt.close()
     eng_t.close()
 

@@ -22,9 +22,11 @@ f*2/fs, phase (src/gabor.cpp:123-130).
 """
 from __future__ import annotations
 
+import atexit
 import ctypes
 import math
 import os
+import weakref
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -83,7 +85,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     global _lib
     if _lib is not None:
         return _lib
-    p = path or LIB_PATH
+    p = path or os.environ.get("EMPI_B200_LIB") or LIB_PATH
     if not os.path.exists(p):
         raise OSError(f"{p} is missing: build it with `python -m empi_b200.build`")
     L = ctypes.CDLL(p)
@@ -179,9 +181,18 @@ class Engine:
         _check(L.empi_engine_create(ctypes.byref(o), ctypes.byref(h)))
         self.handle = h
         self.opts = o
+        self._children = weakref.WeakSet()
+        _live_engines.add(self)
+
+    def _adopt(self, child):
+        self._children.add(child)
 
     def close(self):
-        if self.handle:
+        """Destroys the engine after every workspace and batch created on it
+        (the C ABI requires children to go first)."""
+        if getattr(self, "handle", None):
+            for c in list(self._children):
+                c.close()
             load_library().empi_engine_destroy(self.handle)
             self.handle = None
 
@@ -193,6 +204,17 @@ class Engine:
 
 
 _default_engine = None
+_live_engines = weakref.WeakSet()
+
+
+@atexit.register
+def _close_all():
+    # release device objects before the interpreter (and the CUDA runtime) tear down
+    for e in list(_live_engines):
+        try:
+            e.close()
+        except Exception:
+            pass
 
 
 def default_engine() -> Engine:
@@ -269,11 +291,12 @@ class GaborWorkspace:
         h = ctypes.c_void_p()
         _check(L.empi_workspace_create(self.engine.handle, ctypes.byref(d), fs, C, N, variant, ctypes.byref(h)))
         self.handle = h
+        self.engine._adopt(self)
 
     def close(self):
-        if getattr(self, "handle", None):
+        if getattr(self, "handle", None) and getattr(self.engine, "handle", None):
             load_library().empi_workspace_destroy(self.handle)
-            self.handle = None
+        self.handle = None
 
     def __del__(self):
         try:
@@ -360,11 +383,12 @@ class Batch:
         _check(L.empi_batch_create(self.engine.handle, self.variant, ctypes.byref(d), ctypes.byref(s), eps,
                                    len(self.shapes), ctypes.byref(h)))
         self.handle = h
+        self.engine._adopt(self)
 
     def close(self):
-        if getattr(self, "handle", None):
+        if getattr(self, "handle", None) and getattr(self.engine, "handle", None):
             load_library().empi_batch_destroy(self.handle)
-            self.handle = None
+        self.handle = None
 
     def __del__(self):
         try:

@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
                      "--expt-relaxed-constexpr", "-diag-suppress", "177"]
 SOURCES = ["engine.cu", "geometry.cpp", "hostio.cpp"]
-HEADERS = ["fft.cuh", "kernels.cuh", "plan.hpp", "geometry.hpp", "engine.hpp"]
+HEADERS = ["fft.cuh", "kernels.cuh", "refresh.cuh", "plan.hpp", "geometry.hpp", "engine.hpp"]
 
 
 def nvcc() -> str:

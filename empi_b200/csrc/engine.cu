@@ -44,7 +44,7 @@ empi_status ok() {
         if (e_ != cudaSuccess) {                                                           \
             return fail(e_ == cudaErrorMemoryAllocation ? EMPI_ERR_OUT_OF_MEMORY : EMPI_ERR_CUDA, \
                         e_ == cudaErrorMemoryAllocation ? std::string("insufficientMemory")  \
-                                                        : std::string("cuda: ") + cudaGetErrorString(e_)); \
+                                                        : std::string("cuda: ") + cudaGetErrorString(e_) + " (" #expr ")"); \
         }                                                                                  \
     } while (0)
 
@@ -72,6 +72,8 @@ extern "C" const char* empi_status_string(empi_status st) {
 
 // ------------------------------------------------------------ engine
 
+constexpr int kSizes = 13;  // sub-FFT sizes 2^0 .. 2^12, one refresh kernel each
+
 struct empi_engine {
     empi_engine_opts opts;
     int device = 0;
@@ -79,6 +81,8 @@ struct empi_engine {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     float2* tw = nullptr;
+    cudaStream_t aux[kSizes] = {};     // branches of the per-size refresh fork
+    cudaEvent_t fork = nullptr, join[kSizes] = {};
 };
 
 extern "C" void empi_engine_opts_default(empi_engine_opts* o) {
@@ -133,6 +137,11 @@ extern "C" empi_status empi_engine_create(const empi_engine_opts* opts, empi_eng
     }
     CUDA_TRY(cudaMalloc(&e->tw, sizeof(float2) * kTwN));
     CUDA_TRY(cudaMemcpy(e->tw, tw.data(), sizeof(float2) * kTwN, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
+    for (int i = 0; i < kSizes; ++i) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&e->aux[i], cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming));
+    }
     *out = e.release();
     return ok();
 }
@@ -141,6 +150,11 @@ extern "C" void empi_engine_destroy(empi_engine* e) {
     if (!e) return;
     cudaSetDevice(e->device);
     if (e->tw) cudaFree(e->tw);
+    for (int i = 0; i < kSizes; ++i) {
+        if (e->aux[i]) cudaStreamDestroy(e->aux[i]);
+        if (e->join[i]) cudaEventDestroy(e->join[i]);
+    }
+    if (e->fork) cudaEventDestroy(e->fork);
     if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }
@@ -152,9 +166,10 @@ extern "C" empi_status empi_dictionary_size(const empi_dictionary* d, double fs,
     if (!d) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
     DictPlan dp;
     std::vector<ScalePlan> sp;
+    std::vector<float> et;
     std::string err;
-    if (!build_dictionary(fs, samples, d->energy_error, d->scale_min, d->scale_max, d->freq_max, 4096, dp, sp,
-                          err))
+    if (!build_dictionary(fs, samples, d->energy_error, d->scale_min, d->scale_max, d->freq_max, 4096, dp, sp, et,
+                          nullptr, nullptr, err))
         return fail(err == "signalFileIsTooLongForThisDecomposition" ? EMPI_ERR_SIGNAL_TOO_LONG
                                                                      : EMPI_ERR_INVALID_ARGUMENT,
                     err);
@@ -168,9 +183,10 @@ extern "C" empi_status empi_dictionary_scales(const empi_dictionary* d, double f
     if (!d) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
     DictPlan dp;
     std::vector<ScalePlan> sp;
+    std::vector<float> et;
     std::string err;
-    if (!build_dictionary(fs, samples, d->energy_error, d->scale_min, d->scale_max, d->freq_max, 4096, dp, sp,
-                          err))
+    if (!build_dictionary(fs, samples, d->energy_error, d->scale_min, d->scale_max, d->freq_max, 4096, dp, sp, et,
+                          nullptr, nullptr, err))
         return fail(EMPI_ERR_INVALID_ARGUMENT, err);
     for (int i = 0; i < dp.nscales && i < cap; ++i) {
         if (s) s[i] = sp[i].s;
@@ -207,6 +223,9 @@ struct empi_batch {
     empi_settings settings{};
     std::vector<DictPlan> dicts;
     std::vector<ScalePlan> scales;
+    std::vector<float> etab;
+    std::vector<WinGeom> wgeom;
+    std::vector<float> whf;
     std::vector<InstPlan> insts;
     std::vector<int2> blk_ic;
     std::vector<int2> fit_map;      // MMP2: (instance, input channel)
@@ -222,7 +241,8 @@ struct empi_batch {
     DevBuf<DictPlan> d_dicts;
     DevBuf<InstPlan> d_insts;
     DevBuf<int2> d_blk_ic, d_fit_map;
-    DevBuf<float> d_input;
+    DevBuf<float> d_input, d_residual32, d_etab, d_whf;
+    DevBuf<WinGeom> d_wgeom;
     DevBuf<double> d_residual, d_atoms, d_energies, d_chan_energy, d_fit_atoms, d_stats;
     DevBuf<InstState> d_state;
     DevBuf<unsigned long long> d_slots, d_chunks;
@@ -233,6 +253,11 @@ struct empi_batch {
     DevBuf<double2> d_cbin_v;
     DevBuf<int4> d_indices;
     DevBuf<float> d_dump;
+    DevBuf<int4> d_units;
+    DevBuf<int> d_lmeta;  // loff[16], lcap[16], lcount[16], lhead[16]
+    std::vector<int> sizes;  // sub-FFT sizes (log2) present in the batch
+    void* refresh_fn[kSizes] = {};
+    void* collect_fn = nullptr;
 
     BatchDev dev{};
     int refresh_grid = 0, collect_grid = 0, tree_grid = 0, rescore_grid = 0;
@@ -257,17 +282,48 @@ struct empi_batch {
 
 namespace {
 
+template <int MODE, int LG>
+void* refresh_kernel() {
+    return (void*)k_refresh<MODE, LG>;
+}
+
+template <int MODE>
+void* refresh_kernel_of(int lg) {
+    switch (lg) {
+        case 0: return refresh_kernel<MODE, 0>();
+        case 1: return refresh_kernel<MODE, 1>();
+        case 2: return refresh_kernel<MODE, 2>();
+        case 3: return refresh_kernel<MODE, 3>();
+        case 4: return refresh_kernel<MODE, 4>();
+        case 5: return refresh_kernel<MODE, 5>();
+        case 6: return refresh_kernel<MODE, 6>();
+        case 7: return refresh_kernel<MODE, 7>();
+        case 8: return refresh_kernel<MODE, 8>();
+        case 9: return refresh_kernel<MODE, 9>();
+        case 10: return refresh_kernel<MODE, 10>();
+        case 11: return refresh_kernel<MODE, 11>();
+        default: return refresh_kernel<MODE, 12>();
+    }
+}
+
 template <int MODE>
 empi_status configure_refresh(empi_batch* b) {
     const size_t smem = refresh_smem_bytes<MODE>();
-    CUDA_TRY(cudaFuncSetAttribute(k_refresh<MODE, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    CUDA_TRY(cudaFuncSetAttribute(k_refresh<MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int occ = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_refresh<MODE, false>, kUnitThreads, smem));
-    if (occ < 1) return fail(EMPI_ERR_INTERNAL, "refreshKernelDoesNotFit");
+    int occ = 1 << 30;
+    for (int lg : b->sizes) {
+        void* fn = refresh_kernel_of<MODE>(lg);
+        CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int o = 0;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fn, kUnitThreads, smem));
+        occ = std::min(occ, o);
+        b->refresh_fn[lg] = fn;
+    }
+    b->collect_fn = (void*)k_collect<MODE>;
+    CUDA_TRY(cudaFuncSetAttribute(b->collect_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (occ < 1 || occ == (1 << 30)) return fail(EMPI_ERR_INTERNAL, "refreshKernelDoesNotFit");
     b->refresh_smem = smem;
     b->refresh_grid = b->eng->sms * occ;
-    b->collect_grid = b->eng->sms * occ;
+    b->collect_grid = b->eng->sms;
     return EMPI_OK;
 }
 
@@ -279,22 +335,27 @@ empi_status configure(empi_batch* b) {
     }
 }
 
-void launch_refresh(empi_batch* b, bool collect, cudaStream_t s) {
-    const dim3 grid(collect ? b->collect_grid : b->refresh_grid), block(kUnitThreads);
-    switch (b->mode) {
-        case MODE_SINGLE:
-            if (collect) k_refresh<MODE_SINGLE, true><<<grid, block, b->refresh_smem, s>>>(b->dev);
-            else k_refresh<MODE_SINGLE, false><<<grid, block, b->refresh_smem, s>>>(b->dev);
-            break;
-        case MODE_MMP1:
-            if (collect) k_refresh<MODE_MMP1, true><<<grid, block, b->refresh_smem, s>>>(b->dev);
-            else k_refresh<MODE_MMP1, false><<<grid, block, b->refresh_smem, s>>>(b->dev);
-            break;
-        default:
-            if (collect) k_refresh<MODE_MMP3, true><<<grid, block, b->refresh_smem, s>>>(b->dev);
-            else k_refresh<MODE_MMP3, false><<<grid, block, b->refresh_smem, s>>>(b->dev);
-            break;
+// the per-size refresh kernels as parallel branches: fork from s, join into s
+void launch_refresh(empi_batch* b, cudaStream_t s) {
+    empi_engine* e = b->eng;
+    void* args[] = {&b->dev};
+    if (b->sizes.size() == 1) {
+        cudaLaunchKernel(b->refresh_fn[b->sizes[0]], dim3(b->refresh_grid), dim3(kUnitThreads), args, b->refresh_smem, s);
+        return;
     }
+    cudaEventRecord(e->fork, s);
+    for (size_t i = 0; i < b->sizes.size(); ++i) {
+        cudaStreamWaitEvent(e->aux[i], e->fork, 0);
+        cudaLaunchKernel(b->refresh_fn[b->sizes[i]], dim3(b->refresh_grid), dim3(kUnitThreads), args,
+                         b->refresh_smem, e->aux[i]);
+        cudaEventRecord(e->join[i], e->aux[i]);
+    }
+    for (size_t i = 0; i < b->sizes.size(); ++i) cudaStreamWaitEvent(s, e->join[i], 0);
+}
+
+void launch_collect(empi_batch* b, cudaStream_t s) {
+    void* args[] = {&b->dev};
+    cudaLaunchKernel(b->collect_fn, dim3(b->collect_grid), dim3(kUnitThreads), args, b->refresh_smem, s);
 }
 
 // schedule + refresh + tree + root (the map update after a subtraction, or
@@ -302,10 +363,11 @@ void launch_refresh(empi_batch* b, bool collect, cudaStream_t s) {
 void launch_update(empi_batch* b, int sched_mode, int only_scale, double tA, double sA, cudaStream_t s,
                    cudaEvent_t e0, cudaEvent_t e1) {
     const int ninst = (int)b->insts.size();
+    cudaMemsetAsync(b->dev.lcount, 0, sizeof(int) * 2 * 16, s);  // lcount and lhead
     k_sched_a<<<ninst, 128, 0, s>>>(b->dev, sched_mode, only_scale, tA, sA);
     k_sched_b<<<1, 1024, 0, s>>>(b->dev);
     if (e0) cudaEventRecord(e0, s);
-    launch_refresh(b, false, s);
+    launch_refresh(b, s);
     if (e1) cudaEventRecord(e1, s);
     k_tree<<<b->tree_grid, 256, 0, s>>>(b->dev);
     k_root<<<ninst, 256, 0, s>>>(b->dev);
@@ -315,7 +377,7 @@ void launch_update(empi_batch* b, int sched_mode, int only_scale, double tA, dou
 void launch_select(empi_batch* b, cudaStream_t s) {
     const int ninst = (int)b->insts.size();
     k_cand_slots<<<ninst, 256, 0, s>>>(b->dev);
-    launch_refresh(b, true, s);
+    launch_collect(b, s);
     k_rescore<<<b->rescore_grid, 128, 0, s>>>(b->dev);
     k_select<<<ninst, 128, 0, s>>>(b->dev);
 }
@@ -352,7 +414,8 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
             DictPlan dp;
             std::string err;
             if (!build_dictionary(ep.fs, ep.samples, dict->energy_error, dict->scale_min, dict->scale_max,
-                                  dict->freq_max, eng->opts.transform_cap, dp, b->scales, err))
+                                  dict->freq_max, eng->opts.transform_cap, dp, b->scales, b->etab, &b->wgeom,
+                                  &b->whf, err))
                 return fail(err == "signalFileIsTooLongForThisDecomposition" ? EMPI_ERR_SIGNAL_TOO_LONG
                                                                              : EMPI_ERR_INVALID_ARGUMENT,
                             err);
@@ -411,6 +474,27 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
     }
     b->nij = ij_off;
     const int ninst = (int)b->insts.size();
+    // per sub-FFT size: the units of a full pass (the most a round can append)
+    long long lcapl[16] = {0};
+    for (const InstPlan& ip : b->insts) {
+        const DictPlan& dp = b->dicts[ip.dict];
+        for (int j = 0; j < dp.nscales; ++j) {
+            const ScalePlan& sp = b->scales[dp.scale0 + j];
+            for (int g = 0; g < sp.G; ++g) {
+                const int B = g >= 2 ? sp.B2 : sp.B1;
+                lcapl[sp.logL] += (sp.tcount + B - 1) / B;
+            }
+        }
+    }
+    int lmeta[64] = {0};
+    long long lsum = 0;
+    for (int l = 0; l < 16; ++l) {
+        if (lcapl[l] > 0 && l < kSizes) b->sizes.push_back(l);
+        lmeta[l] = (int)lsum;
+        lmeta[16 + l] = (int)lcapl[l];
+        lsum += lcapl[l];
+    }
+    if (lsum > (1LL << 31) - 1) return fail(EMPI_ERR_SIGNAL_TOO_LONG, "batchTooLarge");
     const int band_cap = eng->opts.candidate_capacity > 0 ? eng->opts.candidate_capacity
                                                           : std::max(8192, 64 * ninst);
     CUDA_TRY(b->d_scales.alloc(b->scales.size()));
@@ -420,6 +504,10 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
     CUDA_TRY(b->d_fit_map.alloc(b->fit_map.size()));
     CUDA_TRY(b->d_input.alloc(b->total_in));
     CUDA_TRY(b->d_residual.alloc(res_off));
+    CUDA_TRY(b->d_residual32.alloc(res_off));
+    CUDA_TRY(b->d_etab.alloc(b->etab.size()));
+    CUDA_TRY(b->d_wgeom.alloc(b->wgeom.size()));
+    CUDA_TRY(b->d_whf.alloc(b->whf.size()));
     CUDA_TRY(b->d_atoms.alloc(out_off));
     CUDA_TRY(b->d_energies.alloc((size_t)ninst * iters));
     CUDA_TRY(b->d_chan_energy.alloc(cen_off));
@@ -441,11 +529,19 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
     const int inst_bin_cap = 512;
     CUDA_TRY(b->d_inst_bins.alloc((size_t)ninst * inst_bin_cap));
     CUDA_TRY(b->d_indices.alloc((size_t)ninst * iters));
+    CUDA_TRY(b->d_units.alloc((size_t)lsum));
+    CUDA_TRY(b->d_lmeta.alloc(64));
     cudaStream_t s = eng->stream;
     CUDA_TRY(cudaMemcpyAsync(b->d_scales.p, b->scales.data(), sizeof(ScalePlan) * b->scales.size(),
                              cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaMemcpyAsync(b->d_dicts.p, b->dicts.data(), sizeof(DictPlan) * b->dicts.size(),
                              cudaMemcpyHostToDevice, s));
+    if (!b->etab.empty())
+        CUDA_TRY(cudaMemcpyAsync(b->d_etab.p, b->etab.data(), sizeof(float) * b->etab.size(), cudaMemcpyHostToDevice,
+                                 s));
+    CUDA_TRY(cudaMemcpyAsync(b->d_wgeom.p, b->wgeom.data(), sizeof(WinGeom) * b->wgeom.size(), cudaMemcpyHostToDevice,
+                             s));
+    CUDA_TRY(cudaMemcpyAsync(b->d_whf.p, b->whf.data(), sizeof(float) * b->whf.size(), cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaMemcpyAsync(b->d_insts.p, b->insts.data(), sizeof(InstPlan) * ninst, cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaMemcpyAsync(b->d_blk_ic.p, b->blk_ic.data(), sizeof(int2) * b->blk_ic.size(),
                              cudaMemcpyHostToDevice, s));
@@ -455,6 +551,7 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
     CUDA_TRY(cudaMemsetAsync(b->d_chunks.p, 0, sizeof(unsigned long long) * b->d_chunks.n, s));
     CUDA_TRY(cudaMemsetAsync(b->d_slots.p, 0, sizeof(unsigned long long) * b->d_slots.n, s));
     CUDA_TRY(cudaMemsetAsync(b->d_ctr.p, 0, sizeof(int) * CTR_COUNT, s));
+    CUDA_TRY(cudaMemcpyAsync(b->d_lmeta.p, lmeta, sizeof(lmeta), cudaMemcpyHostToDevice, s));
 
     BatchDev& d = b->dev;
     d.scales = b->d_scales.p;
@@ -474,6 +571,15 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
     d.cbin_cap = band_cap;
     d.inst_bin_cap = inst_bin_cap;
     d.residual = b->d_residual.p;
+    d.residual32 = b->d_residual32.p;
+    d.etab = b->d_etab.p;
+    d.wtab = reinterpret_cast<const int4*>(b->d_wgeom.p);
+    d.whf = b->d_whf.p;
+    d.units = b->d_units.p;
+    d.loff = b->d_lmeta.p;
+    d.lcap = b->d_lmeta.p + 16;
+    d.lcount = b->d_lmeta.p + 32;
+    d.lhead = b->d_lmeta.p + 48;
     d.state = b->d_state.p;
     d.slots = b->d_slots.p;
     d.chunks = b->d_chunks.p;
@@ -530,18 +636,17 @@ empi_status check_errors(empi_batch* b) {
 }
 
 empi_status capture_graph(empi_batch* b) {
-    if (b->graph) return EMPI_OK;
     const int K = b->eng->opts.iterations_per_graph;
-    cudaStream_t s = b->eng->stream;
     const bool timing = b->eng->opts.timing != 0;
     if (timing && b->ev.empty()) {
         b->ev.resize(2 * (K + 1));
         for (auto& e : b->ev) CUDA_TRY(cudaEventCreate(&e));
     }
+    if (b->graph || timing) return EMPI_OK;  // timing mode launches eagerly, events between kernels
+    cudaStream_t s = b->eng->stream;
     cudaGraph_t g = nullptr;
     CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < K; ++k)
-        launch_iteration(b, s, timing ? b->ev[2 * (k + 1)] : nullptr, timing ? b->ev[2 * (k + 1) + 1] : nullptr);
+    for (int k = 0; k < K; ++k) launch_iteration(b, s, nullptr, nullptr);
     cudaError_t ce = cudaStreamEndCapture(s, &g);
     if (ce != cudaSuccess) return fail(EMPI_ERR_CUDA, std::string("cuda: ") + cudaGetErrorString(ce));
     ce = cudaGraphInstantiate(&b->graph, g, 0);
@@ -621,14 +726,20 @@ extern "C" empi_status empi_batch_run(empi_batch* b) {
     int iters = 0;
     const int imax = b->settings.iteration_max;
     int active = 1;
+    const int K = b->eng->opts.iterations_per_graph;
     while (iters < imax && active > 0) {
-        CUDA_TRY(cudaGraphLaunch(b->graph, s));
-        iters += b->graph_iters;
-        launches += b->graph_iters * b->launches_per_iter;
+        if (timing) {
+            for (int k = 0; k < K; ++k) launch_iteration(b, s, b->ev[2 * (k + 1)], b->ev[2 * (k + 1) + 1]);
+            CUDA_TRY(cudaGetLastError());
+        } else {
+            CUDA_TRY(cudaGraphLaunch(b->graph, s));
+        }
+        iters += K;
+        launches += K * b->launches_per_iter;
         CUDA_TRY(cudaMemcpyAsync(&active, b->d_ctr.p + CTR_ACTIVE, sizeof(int), cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaStreamSynchronize(s));
         if (timing) {
-            for (int k = 0; k < b->graph_iters; ++k) {
+            for (int k = 0; k < K; ++k) {
                 float ms = 0.f;
                 CUDA_TRY(cudaEventElapsedTime(&ms, b->ev[2 * (k + 1)], b->ev[2 * (k + 1) + 1]));
                 refresh_ms += ms;
@@ -885,7 +996,7 @@ extern "C" empi_status empi_workspace_subtract_atom(empi_workspace* w, const dou
     double* x = b->d_residual.p + (size_t)channel * w->N;
     CUDA_TRY(cudaMemcpyAsync(x, samples, sizeof(double) * w->N, cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaMemcpyAsync(w->d_params, params, sizeof(double) * 6, cudaMemcpyHostToDevice, s));
-    k_subtract_signal<<<1, 256, 0, s>>>(x, w->N, w->fs, w->d_params, 0);
+    k_subtract_signal<<<1, 256, 0, s>>>(x, b->d_residual32.p + (size_t)channel * w->N, w->N, w->fs, w->d_params, 0);
     CUDA_TRY(cudaMemcpyAsync(samples, x, sizeof(double) * w->N, cudaMemcpyDeviceToHost, s));
     st = ws_reset_state(w);
     if (st != EMPI_OK) return st;
@@ -930,7 +1041,7 @@ extern "C" empi_status empi_subtract_atom_from_signal(empi_engine* eng, double* 
     cudaStream_t s = eng->stream;
     CUDA_TRY(cudaMemcpyAsync(x.p, samples, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaMemcpyAsync(p.p, params, sizeof(double) * 6, cudaMemcpyHostToDevice, s));
-    k_subtract_signal<<<1, 256, 0, s>>>(x.p, n, fs, p.p, fit);
+    k_subtract_signal<<<1, 256, 0, s>>>(x.p, nullptr, n, fs, p.p, fit);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(samples, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaMemcpyAsync(params, p.p, sizeof(double) * 6, cudaMemcpyDeviceToHost, s));

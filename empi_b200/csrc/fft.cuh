@@ -81,22 +81,19 @@ template <int R, int VPT, int TW_N>
 __device__ __forceinline__ void fft_pass(float2* buf, int logL, int logNs, int points,
                                          const float2* __restrict__ tw) {
     constexpr int JPT = VPT / R;
-    const int L = 1 << logL;
+    constexpr int logR = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4;
     const int Ns = 1 << logNs;
-    const int logQ = logL - (R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4);
+    const int logQ = logL - logR;
     const int Q = 1 << logQ;  // L / R
-    const int jobs = points / R;
-    const int twShift = TW_N / (Ns * R);
+    const int jobs = points >> logR;
+    const int twShift = TW_N >> (logNs + logR);
     float2 v[JPT][R];
-    int obase[JPT];
 #pragma unroll
     for (int jj = 0; jj < JPT; ++jj) {
         const int job = threadIdx.x + jj * blockDim.x;
-        obase[jj] = -1;
         if (job < jobs) {
-            const int f = job >> logQ;
             const int j = job & (Q - 1);
-            const int base = f << logL;
+            const int base = (job >> logQ) << logL;
 #pragma unroll
             for (int r = 0; r < R; ++r) v[jj][r] = buf[pad16(base + j + r * Q)];
             const int k = j & (Ns - 1);
@@ -105,15 +102,18 @@ __device__ __forceinline__ void fft_pass(float2* buf, int logL, int logNs, int p
                 for (int r = 1; r < R; ++r) v[jj][r] = cmul(v[jj][r], __ldg(tw + k * r * twShift));
             }
             dft<R>(v[jj]);
-            obase[jj] = base + (j - k) * R + k;
         }
     }
     __syncthreads();
 #pragma unroll
     for (int jj = 0; jj < JPT; ++jj) {
-        if (obase[jj] >= 0) {
+        const int job = threadIdx.x + jj * blockDim.x;
+        if (job < jobs) {
+            const int j = job & (Q - 1);
+            const int k = j & (Ns - 1);
+            const int ob = ((job >> logQ) << logL) + (j - k) * R + k;
 #pragma unroll
-            for (int r = 0; r < R; ++r) buf[pad16(obase[jj] + r * Ns)] = v[jj][r];
+            for (int r = 0; r < R; ++r) buf[pad16(ob + r * Ns)] = v[jj][r];
         }
     }
     __syncthreads();
@@ -140,6 +140,17 @@ __device__ __forceinline__ void fft_batch(float2* buf, int logL, int points, con
         fft_pass<16, VPT, TW_N>(buf, logL, logNs, points, tw);
         logNs += 4;
     }
+}
+
+// Same as fft_batch with the size fixed at compile time.
+template <int VPT, int TW_N, int LOGL>
+__device__ __forceinline__ void fft_batch_t(float2* buf, int points, const float2* __restrict__ tw) {
+    constexpr int first = LOGL & 3;
+    if constexpr (first == 1) fft_pass<2, VPT, TW_N>(buf, LOGL, 0, points, tw);
+    if constexpr (first == 2) fft_pass<4, VPT, TW_N>(buf, LOGL, 0, points, tw);
+    if constexpr (first == 3) fft_pass<8, VPT, TW_N>(buf, LOGL, 0, points, tw);
+#pragma unroll
+    for (int logNs = first; logNs < LOGL; logNs += 4) fft_pass<16, VPT, TW_N>(buf, LOGL, logNs, points, tw);
 }
 
 }  // namespace empi

@@ -28,6 +28,7 @@ int ilog2(long x) {
 
 bool build_dictionary(double fs, int N, double energyError, double scaleMin, double scaleMax,
                       double freqMax, int lcap, DictPlan& dict, std::vector<ScalePlan>& scales,
+                      std::vector<float>& etab, std::vector<WinGeom>* wgeom, std::vector<float>* whf,
                       std::string& err) {
     if (!(fs > 0.0) || !std::isfinite(fs)) {
         err = "invalidSamplingFrequency";
@@ -97,13 +98,22 @@ bool build_dictionary(double fs, int N, double energyError, double scaleMin, dou
         p.fcount = (int)fCount;
         p.tcount = (int)tCount;
 
-        // longest window over the time grid (src/gabor.cpp:279-292)
+        // window of every t (src/gabor.cpp:279-292) and the longest one
         int wmax = 1;
+        p.win_base = wgeom ? (long long)wgeom->size() : 0;
         for (long ti = 0; ti < tCount; ++ti) {
             const double t0 = ti * tMax / (tCount - 1);
             long l = std::lrint((t0 - hw) * fs), r = std::lrint((t0 + hw) * fs);
             long iL = std::max(0L, l), iR = std::min((long)N - 1, r);
             wmax = std::max(wmax, (int)(iR - iL + 1));
+            if (wgeom) {
+                const double t0fixed = t0 - iL / fs;
+                const double c = t0fixed * fs;
+                const double cfl = std::floor(c);
+                wgeom->push_back(WinGeom{(int)iL, (int)(iR - iL + 1), (int)cfl, (float)(c - cfl)});
+                const double ft = fs * t0;
+                whf->push_back((float)(ft - std::rint(ft)));
+            }
         }
         if (wmax > Nfft) {
             // the reference would write past its FFT buffer here
@@ -152,10 +162,21 @@ bool build_dictionary(double fs, int N, double energyError, double scaleMin, dou
         p.klo = klo;
         p.khi = khi;
         p.khf = khf;
+        // expFactor (src/gabor.cpp:51) of the phase-dependent bins, FP64 -> FP32
+        p.eoff = (int)etab.size();
+        auto efac = [&](long k) {
+            double f = k * fs / Nfft;
+            bool high = f > 0.5 * nyq;
+            double f4 = high ? (nyq - f) : f;
+            return (float)std::exp(-2 * M_PI * s * s * f4 * f4);
+        };
+        for (long k = 0; k < klo; ++k) etab.push_back(efac(k));
+        for (long k = khi + 1; k < fCount; ++k) etab.push_back(efac(k));
         p.slot_base = slots;
         p.aG = (float)(std::sqrt(M_PI) / (s * fs));
         p.Kc = (float)(2.0 * M_SQRT2 / (s * fs));
         p.K1 = (float)(M_SQRT2 / (s * fs));
+        p.aG2 = (float)(std::sqrt(M_PI) / (s * fs) * std::sqrt(1.0 / std::log(2.0)));
         slots += (long long)tCount * p.G;
         values += (unsigned long long)fCount * (unsigned long long)tCount;
         scales.push_back(p);

@@ -69,12 +69,6 @@ struct CandBin {
     double e64;
 };
 
-struct WinMeta {
-    double c64, fst0;
-    int iL, W, ci;
-    float cf;
-};
-
 struct BatchDev {
     const ScalePlan* scales;
     const DictPlan* dicts;
@@ -87,6 +81,15 @@ struct BatchDev {
     float band;
     int cslot_cap, cbin_cap, inst_bin_cap;
     double* residual;
+    float* residual32;    // FP32 copy of the residual read by the refresh loads
+    const float* etab;    // per-scale expFactor of the phase-dependent bins
+    const int4* wtab;     // per-window (iL, W, ci, cf bits), WinGeom
+    const float* whf;     // per-window fs t0 modulo 1 in [-0.5, 0.5)
+    int4* units;          // refresh work units, one list per sub-FFT size: (inst, j | g << 16, t0, nwin)
+    const int* loff;      // per size: offset of its list in units
+    const int* lcap;      // per size: capacity of its list
+    int* lcount;          // per size: units appended this round (reset before the schedule)
+    int* lhead;           // per size: work-queue head (reset before the schedule)
     InstState* state;
     unsigned long long* slots;
     unsigned long long* chunks;
@@ -180,380 +183,7 @@ __device__ __forceinline__ float2 twiddle_frac(long long a, long long b, const f
     return make_float2(c, s);
 }
 
-// Energy of one channel's spectral value X (unnormalised FFT bin) at bin k:
-// fs |v|^2 normReal^2 with v = X e^{i theta_k} / fs, GaborComputer::compute
-// (src/gabor.cpp:54-71) in closed form: K |X|^4 / (|X|^2 + e Re(X^2 e^{i psi})).
-__device__ __forceinline__ float phase_turns(int k, const ScalePlan& sp, const WinMeta& m, bool high) {
-    double tt = 2.0 * (double)k * m.c64 / (double)sp.nfft;
-    if (high) tt -= m.fst0;
-    tt -= rint(tt);
-    return (float)tt;
-}
-
-__device__ __forceinline__ float exp_factor(int k, const ScalePlan& sp, double fs, bool high) {
-    double f = (double)k * fs / (double)sp.nfft;
-    double f4 = high ? (0.5 * fs - f) : f;
-    return (float)exp(-2 * CUDART_PI * sp.s * sp.s * f4 * f4);
-}
-
-__device__ __forceinline__ float energy_one(float2 X, int k, const ScalePlan& sp, const WinMeta& m, double fs) {
-    const float p = X.x * X.x + X.y * X.y;
-    if (k < sp.klo || k > sp.khi) {
-        const bool high = k >= sp.khf;
-        const float e = exp_factor(k, sp, fs, high);
-        float sn, cs;
-        sincospif(2.0f * phase_turns(k, sp, m, high), &sn, &cs);
-        const float re = (X.x * X.x - X.y * X.y) * cs - 2.0f * X.x * X.y * sn;
-        const float D = p + e * re;
-        return (D > 0.0f && p > 0.0f) ? sp.Kc * p * (p / D) : 0.0f;
-    }
-    return sp.Kc * p;
-}
-
-// MMP1 closed form (constraint + normalisation, src/mmp.cpp:9-21 with
-// src/gabor.cpp:54-71) from P = sum |X_c|^2 and S = sum X_c^2.
-__device__ __forceinline__ float energy_mmp1(float P, float2 S, int k, const ScalePlan& sp, const WinMeta& m,
-                                             double fs) {
-    const float as = sqrtf(S.x * S.x + S.y * S.y);
-    if (k < sp.klo || k > sp.khi) {
-        const float e = exp_factor(k, sp, fs, false);
-        if (as == 0.0f) return sp.K1 * P / (1.0f + e);
-        float sn, cs;
-        sincospif(2.0f * phase_turns(k, sp, m, false), &sn, &cs);
-        const float re = S.x * cs - S.y * sn;
-        const float D = as + e * re;
-        return D > 0.0f ? sp.K1 * (P + as) * (as / D) : 0.0f;
-    }
-    return sp.K1 * (P + as);
-}
-
-// Segmented max over consecutive lanes that share a window, then one shared
-// atomic per segment head.
-__device__ __forceinline__ void seg_max_flush(unsigned long long key, int w, unsigned long long* wkey) {
-    const unsigned lane = threadIdx.x & 31;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        unsigned long long ok = __shfl_down_sync(0xffffffffu, key, off);
-        int ow = __shfl_down_sync(0xffffffffu, w, off);
-        if (lane + off < 32 && ow == w && ok > key) key = ok;
-    }
-    int pw = __shfl_up_sync(0xffffffffu, w, 1);
-    if (w >= 0 && (lane == 0 || pw != w)) atomicMax(wkey + w, key);
-}
-
-// ------------------------------------------------------------ refresh
-
-constexpr int kVPT = kUnitPoints / kUnitThreads;
-constexpr int kBufFloat2 = kUnitPoints + kUnitPoints / 16 + 16;
-constexpr int kAccBins = kUnitPoints + kMaxWindowsPerUnit;
-
-template <int MODE>
-constexpr size_t refresh_smem_bytes() {
-    return sizeof(float2) * kBufFloat2 + sizeof(WinMeta) * kMaxWindowsPerUnit +
-           sizeof(unsigned long long) * kMaxWindowsPerUnit +
-           (MODE == MODE_SINGLE ? 0 : sizeof(float) * kAccBins * (MODE == MODE_MMP1 ? 3 : 1));
-}
-
-template <int MODE, bool COLLECT>
-__device__ void process_unit(const BatchDev& b, unsigned char* smem, int inst, int j, int g, int t_start,
-                             int nwin, unsigned thr_bits) {
-    float2* buf = reinterpret_cast<float2*>(smem);
-    WinMeta* meta = reinterpret_cast<WinMeta*>(smem + sizeof(float2) * kBufFloat2);
-    unsigned long long* wkey = reinterpret_cast<unsigned long long*>(
-        smem + sizeof(float2) * kBufFloat2 + sizeof(WinMeta) * kMaxWindowsPerUnit);
-    float* acc = reinterpret_cast<float*>(smem + sizeof(float2) * kBufFloat2 + sizeof(WinMeta) * kMaxWindowsPerUnit +
-                                          sizeof(unsigned long long) * kMaxWindowsPerUnit);
-
-    const InstPlan ip = b.insts[inst];
-    const DictPlan dp = b.dicts[ip.dict];
-    const ScalePlan sp = b.scales[dp.scale0 + j];
-    const double fs = dp.fs;
-    const int L = sp.L, logL = sp.logL, M = sp.M, F = sp.F;
-    const int Nh = sp.nfft >> 1;
-    const bool pair = g >= 2;
-    const int nf = pair ? 2 : 1;
-    const int nb = g == 0 ? L + 1 : (pair ? 2 * L : L);
-    const int r = g == 0 ? 0 : (g == 1 ? M / 2 : g - 1);
-    const int tid = threadIdx.x, T = blockDim.x;
-
-    for (int w = tid; w < nwin; w += T) {
-        const int ti = t_start + w;
-        const double t0 = grid_t(ti, dp.tMax, sp.tcount);
-        int iL, iR;
-        double t0fixed;
-        window_bounds(t0, sp.hw, fs, dp.N, iL, iR, t0fixed);
-        WinMeta m;
-        m.c64 = t0fixed * fs;
-        m.fst0 = fs * t0;
-        m.iL = iL;
-        m.W = iR - iL + 1;
-        const double cfl = floor(m.c64);
-        m.ci = (int)cfl;
-        m.cf = (float)(m.c64 - cfl);
-        meta[w] = m;
-        wkey[w] = 0ull;
-    }
-    // W_Nfft^rho for the residues of this group
-    float2 wr0, wr1 = make_float2(1.f, 0.f);
-    {
-        float s0, c0;
-        sincospif(-2.0f * (float)r / (float)sp.nfft, &s0, &c0);
-        wr0 = make_float2(c0, s0);
-        if (pair) {
-            sincospif(-2.0f * (float)(M - r) / (float)sp.nfft, &s0, &c0);
-            wr1 = make_float2(c0, s0);
-        }
-    }
-    const int nbins = nwin * nb;
-    if (MODE != MODE_SINGLE) {
-        for (int i = tid; i < nbins * (MODE == MODE_MMP1 ? 3 : 1); i += T) acc[i] = 0.0f;
-    }
-    __syncthreads();
-
-    const int twL = kTwN >> logL;          // table stride for W_L
-    const int tw2L = (kTwN / 2) >> logL;   // table stride for W_{2L}
-    for (int c = 0; c < ip.C; ++c) {
-        const double* x = b.residual + ip.res_off + (long long)c * dp.N;
-        // load: y_r[n'] = sum_m z[n' + mL] W_Nh^{r (n' + mL)}, z[n] = x[2n] g(2n) + i x[2n+1] g(2n+1)
-        const int total = nwin << logL;
-        for (int idx = tid; idx < total; idx += T) {
-            const int w = idx >> logL;
-            const int np = idx & (L - 1);
-            const WinMeta m = meta[w];
-            float2 a1 = make_float2(0.f, 0.f), a2 = make_float2(0.f, 0.f);
-            for (int mm = 0; mm < F; ++mm) {
-                const int n = np + mm * L;
-                const int i0 = 2 * n;
-                if (i0 >= m.W) break;
-                const float x0 = (float)__ldg(x + m.iL + i0);
-                const float x1 = (i0 + 1 < m.W) ? (float)__ldg(x + m.iL + i0 + 1) : 0.0f;
-                const float d0 = (float)(i0 - m.ci) - m.cf;
-                const float y0 = d0 * sp.aG, y1 = (d0 + 1.0f) * sp.aG;
-                const float2 z = make_float2(x0 * expf(-y0 * y0), x1 * expf(-y1 * y1));
-                if (r == 0) {
-                    a1 = cadd(a1, z);
-                } else {
-                    const long long rn = ((long long)r * n) & (Nh - 1);
-                    const float2 tw = twiddle_frac(rn, Nh, b.tw);
-                    a1 = cadd(a1, cmul(z, tw));
-                    if (pair) a2 = cadd(a2, cmulc(z, tw));
-                }
-            }
-            buf[pad16(((w * nf) << logL) + np)] = a1;
-            if (pair) buf[pad16(((w * nf + 1) << logL) + np)] = cmul(a2, __ldg(b.tw + np * twL));
-        }
-        __syncthreads();
-        fft_batch<kVPT, kTwN>(buf, logL, (nwin * nf) << logL, b.tw);
-
-        // post: X[k] = (A + conj(B))/2 - i W_Nfft^k (A - conj(B))/2
-        for (int base = 0; base < nbins; base += T) {
-            const int idx = base + tid;
-            int w = -1, k = 0;
-            float2 X = make_float2(0.f, 0.f);
-            if (idx < nbins) {
-                w = idx / nb;
-                const int jb = idx - w * nb;
-                int q, rho;
-                float2 A, Bq, wr;
-                if (g == 0) {
-                    q = jb;
-                    const int o = w << logL;
-                    A = buf[pad16(o + (q & (L - 1)))];
-                    Bq = buf[pad16(o + ((L - q) & (L - 1)))];
-                    rho = 0;
-                    wr = make_float2(1.f, 0.f);
-                } else if (g == 1) {
-                    q = jb;
-                    const int o = w << logL;
-                    A = buf[pad16(o + q)];
-                    Bq = buf[pad16(o + L - 1 - q)];
-                    rho = M / 2;
-                    wr = wr0;
-                } else {
-                    const int o0 = (2 * w) << logL, o1 = (2 * w + 1) << logL;
-                    if (jb < L) {
-                        q = jb;
-                        A = buf[pad16(o0 + q)];
-                        Bq = buf[pad16(o1 + L - 1 - q)];
-                        rho = r;
-                        wr = wr0;
-                    } else {
-                        q = jb - L;
-                        A = buf[pad16(o1 + q)];
-                        Bq = buf[pad16(o0 + L - 1 - q)];
-                        rho = M - r;
-                        wr = wr1;
-                    }
-                }
-                k = M * q + rho;
-                if (k < sp.fcount) {
-                    const float2 wk = cmul(wr, __ldg(b.tw + q * tw2L));
-                    const float2 Bc = make_float2(Bq.x, -Bq.y);
-                    const float2 E = make_float2(0.5f * (A.x + Bc.x), 0.5f * (A.y + Bc.y));
-                    const float2 D = make_float2(0.5f * (A.x - Bc.x), 0.5f * (A.y - Bc.y));
-                    const float2 O = make_float2(D.y, -D.x);  // -i D
-                    X = cadd(E, cmul(wk, O));
-                } else {
-                    k = -1;
-                }
-            }
-            if (MODE == MODE_SINGLE) {
-                float e = 0.0f;
-                if (k >= 0 && w >= 0) e = energy_one(X, k, sp, meta[w], fs);
-                const unsigned long long key = (k >= 0 && w >= 0) ? pack_key(e, (unsigned)k) : 0ull;
-                if (!COLLECT && b.dump && k >= 0 && w >= 0) b.dump[(long long)k * sp.tcount + t_start + w] = e;
-                if (COLLECT) {
-                    if (k >= 0 && w >= 0 && __float_as_uint(e) >= thr_bits) {
-                        const int slot = atomicAdd(b.ctr + CTR_CBINS, 1);
-                        if (slot < b.cbin_cap) {
-                            const int li = atomicAdd(&b.state[inst].nbins, 1);
-                            if (li < b.inst_bin_cap) {
-                                CandBin cb;
-                                cb.inst = inst;
-                                cb.j = j;
-                                cb.t = t_start + w;
-                                cb.k = k;
-                                cb.e32 = e;
-                                cb.pad = 0;
-                                cb.e64 = 0.0;
-                                b.cbins[slot] = cb;
-                                b.inst_bins[(long long)inst * b.inst_bin_cap + li] = slot;
-                            } else {
-                                b.state[inst].err = ERR_CAND_OVERFLOW;
-                            }
-                        } else {
-                            b.state[inst].err = ERR_CAND_OVERFLOW;
-                        }
-                    }
-                } else {
-                    seg_max_flush(key, w, wkey);
-                }
-            } else if (k >= 0 && w >= 0) {
-                if (MODE == MODE_MMP3 || k >= sp.khf) {
-                    acc[idx] += energy_one(X, k, sp, meta[w], fs);
-                } else {
-                    acc[idx] += X.x * X.x + X.y * X.y;
-                    acc[nbins + idx] += X.x * X.x - X.y * X.y;
-                    acc[2 * nbins + idx] += 2.0f * X.x * X.y;
-                }
-            }
-        }
-        __syncthreads();
-    }
-
-    if (MODE != MODE_SINGLE) {
-        for (int base = 0; base < nbins; base += T) {
-            const int idx = base + tid;
-            int w = -1, k = -1;
-            float e = 0.0f;
-            if (idx < nbins) {
-                w = idx / nb;
-                const int jb = idx - w * nb;
-                int q, rho;
-                if (g == 0) {
-                    q = jb;
-                    rho = 0;
-                } else if (g == 1) {
-                    q = jb;
-                    rho = M / 2;
-                } else if (jb < L) {
-                    q = jb;
-                    rho = r;
-                } else {
-                    q = jb - L;
-                    rho = M - r;
-                }
-                k = M * q + rho;
-                if (k >= sp.fcount) k = -1;
-                if (k >= 0) {
-                    if (MODE == MODE_MMP3 || k >= sp.khf) {
-                        e = acc[idx];
-                    } else {
-                        e = energy_mmp1(acc[idx], make_float2(acc[nbins + idx], acc[2 * nbins + idx]), k, sp,
-                                        meta[w], fs);
-                    }
-                }
-            }
-            if (COLLECT) {
-                if (k >= 0 && __float_as_uint(e) >= thr_bits) {
-                    const int slot = atomicAdd(b.ctr + CTR_CBINS, 1);
-                    if (slot < b.cbin_cap) {
-                        const int li = atomicAdd(&b.state[inst].nbins, 1);
-                        if (li < b.inst_bin_cap) {
-                            CandBin cb;
-                            cb.inst = inst;
-                            cb.j = j;
-                            cb.t = t_start + w;
-                            cb.k = k;
-                            cb.e32 = e;
-                            cb.pad = 0;
-                            cb.e64 = 0.0;
-                            b.cbins[slot] = cb;
-                            b.inst_bins[(long long)inst * b.inst_bin_cap + li] = slot;
-                        } else {
-                            b.state[inst].err = ERR_CAND_OVERFLOW;
-                        }
-                    } else {
-                        b.state[inst].err = ERR_CAND_OVERFLOW;
-                    }
-                }
-            } else {
-                const unsigned long long key = k >= 0 ? pack_key(e, (unsigned)k) : 0ull;
-                if (b.dump && k >= 0) b.dump[(long long)k * sp.tcount + t_start + w] = e;
-                seg_max_flush(key, k >= 0 ? w : -1, wkey);
-            }
-        }
-        __syncthreads();
-    }
-
-    if (!COLLECT) {
-        unsigned long long* out = b.slots + ip.slot_off + sp.slot_base;
-        for (int w = tid; w < nwin; w += T) out[(long long)(t_start + w) * sp.G + g] = wkey[w];
-    }
-    __syncthreads();
-}
-
-// Persistent refresh: CTAs pull (instance, scale, group, t-batch) units from
-// the schedule's prefix sums; COLLECT pulls candidate slots instead.
-template <int MODE, bool COLLECT>
-__global__ void __launch_bounds__(kUnitThreads, 1) k_refresh(BatchDev b) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int s_unit;
-    const int total = COLLECT ? min(b.ctr[CTR_CSLOTS], b.cslot_cap) : b.ctr[CTR_TOTAL_UNITS];
-    for (;;) {
-        if (threadIdx.x == 0) s_unit = atomicAdd(b.ctr + (COLLECT ? CTR_CSLOT_Q : CTR_UNITS), 1);
-        __syncthreads();
-        const int u = s_unit;
-        __syncthreads();
-        if (u >= total) break;
-        if (COLLECT) {
-            const CandSlot cs = b.cslots[u];
-            const unsigned best = (unsigned)(b.state[cs.inst].best32 >> 32);
-            const float thr = __uint_as_float(best) * (1.0f - b.band);
-            process_unit<MODE, true>(b, smem, cs.inst, cs.j, cs.g, cs.t, 1, __float_as_uint(thr));
-        } else {
-            const int inst = upper_index(b.inst_units, b.ninst, u);
-            int rem = u - b.inst_units[inst];
-            const InstPlan ip = b.insts[inst];
-            const DictPlan dp = b.dicts[ip.dict];
-            const int j = upper_index(b.ij_units + ip.ij_off + inst, dp.nscales, rem);
-            rem -= b.ij_units[ip.ij_off + inst + j];
-            const ScalePlan sp = b.scales[dp.scale0 + j];
-            const int2 dr = b.dirty[ip.ij_off + j];
-            const int n = dr.y - dr.x + 1;
-            int g = 0;
-            for (; g < sp.G; ++g) {
-                const int ng = group_units(n, g, sp);
-                if (rem < ng) break;
-                rem -= ng;
-            }
-            const int B = g >= 2 ? sp.B2 : sp.B1;
-            const int t_start = dr.x + rem * B;
-            const int nwin = min(B, dr.y - t_start + 1);
-            process_unit<MODE, false>(b, smem, inst, j, g, t_start, nwin, 0u);
-        }
-    }
-}
+#include "refresh.cuh"
 
 // ------------------------------------------------------------ schedule
 
@@ -624,6 +254,15 @@ __global__ void k_sched_a(BatchDev b, int mode, int only_scale, double tA_in, do
         if (hi >= lo) {
             const int n = hi - lo + 1;
             for (int g = 0; g < sp.G; ++g) nu += group_units(n, g, sp);
+            // this scale's units go to the list of its sub-FFT size
+            int at = atomicAdd(b.lcount + sp.logL, nu);
+            const int cap = b.lcap[sp.logL];
+            int4* list = b.units + b.loff[sp.logL];
+            for (int g = 0; g < sp.G; ++g) {
+                const int B = g >= 2 ? sp.B2 : sp.B1;
+                for (int t0 = lo; t0 <= hi; t0 += B, ++at)
+                    if (at < cap) list[at] = make_int4(inst, j | (g << 16), t0, min(B, hi - t0 + 1));
+            }
             const long long s0 = sp.slot_base + (long long)lo * sp.G;
             const long long s1 = sp.slot_base + (long long)(hi + 1) * sp.G - 1;
             c0 = (int)(s0 / kChunk);
@@ -799,8 +438,11 @@ __device__ __forceinline__ void slot_to_jtg(const BatchDev& b, const DictPlan& d
 }
 
 // One CTA per instance: every slot whose FP32 max is within the band of the
-// instance's best becomes a candidate (chunks first, then their slots).
+// instance's best becomes a candidate (qualifying chunks first, then their
+// slots).
 __global__ void k_cand_slots(BatchDev b) {
+    __shared__ int s_chunks[256];
+    __shared__ int s_n;
     const int inst = blockIdx.x;
     InstState& st = b.state[inst];
     if (st.status != ST_RUNNING) return;
@@ -815,10 +457,22 @@ __global__ void k_cand_slots(BatchDev b) {
         return;
     }
     const unsigned thr = __float_as_uint(__uint_as_float(best) * (1.0f - b.band));
-    if (threadIdx.x == 0) st.nbins = 0;
-    for (int c = 0; c < dp.chunks; ++c) {
-        const unsigned long long ck = b.chunks[ip.chunk_off + c];
-        if ((unsigned)(ck >> 32) < thr) continue;
+    if (threadIdx.x == 0) {
+        st.nbins = 0;
+        s_n = 0;
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < dp.chunks; c += blockDim.x) {
+        if ((unsigned)(b.chunks[ip.chunk_off + c] >> 32) >= thr) {
+            const int at = atomicAdd(&s_n, 1);
+            if (at < 256) s_chunks[at] = c;
+            else st.err = ERR_CAND_OVERFLOW;
+        }
+    }
+    __syncthreads();
+    const int nc = min(s_n, 256);
+    for (int ic = 0; ic < nc; ++ic) {
+        const int c = s_chunks[ic];
         const long long s0 = (long long)c * kChunk;
         const long long s1 = min(s0 + kChunk, dp.slots);
         for (long long s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
@@ -1115,7 +769,12 @@ __global__ void k_subtract(BatchDev b) {
     const double* p = b.atoms + ip.out_off + ((long long)(st.it - 1) * ip.C + c) * 6;
     const AtomWindow a = atom_window(p, fs, dp.N, false);
     const int Nw = a.iR - a.iL + 1;
-    for (int i = threadIdx.x; i < Nw; i += blockDim.x) x[a.iL + i] -= atom_sample(a, i, fs);
+    float* x32 = b.residual32 + ip.res_off + (long long)c * dp.N;
+    for (int i = threadIdx.x; i < Nw; i += blockDim.x) {
+        const double v = x[a.iL + i] - atom_sample(a, i, fs);
+        x[a.iL + i] = v;
+        x32[a.iL + i] = (float)v;
+    }
     __syncthreads();
     double s = 0.0;
     for (int i = threadIdx.x; i < dp.N; i += blockDim.x) s += x[i] * x[i];
@@ -1150,6 +809,7 @@ __global__ void k_init(BatchDev b, int from_input) {
             v = (double)in[(long long)i * Cin + c];
         }
         if (from_input) x[i] = v;
+        b.residual32[ip.res_off + (long long)c * dp.N + i] = (float)v;
         s += v * v;
     }
     s = block_sum(s, red);
@@ -1168,7 +828,7 @@ __global__ void k_init(BatchDev b, int from_input) {
 
 // Workspace::subtractAtomFromSignal on one FP64 signal (src/gabor.cpp:143-187),
 // fit or not; a single CTA.  params (6) are updated in place when fitting.
-__global__ void k_subtract_signal(double* x, int N, double fs, double* params, int fit) {
+__global__ void k_subtract_signal(double* x, float* x32, int N, double fs, double* params, int fit) {
     __shared__ double red[33];
     double p[6];
     for (int k = 0; k < 6; ++k) p[k] = params[k];
@@ -1190,6 +850,7 @@ __global__ void k_subtract_signal(double* x, int N, double fs, double* params, i
     for (int i = threadIdx.x; i < Nw; i += blockDim.x) {
         const double v = atom_sample(w, i, fs);
         x[w.iL + i] -= fit ? (v / norm) * dot : v;
+        if (x32) x32[w.iL + i] = (float)x[w.iL + i];
     }
     if (fit && threadIdx.x == 0) {
         params[0] = dot;

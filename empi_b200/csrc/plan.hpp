@@ -39,10 +39,20 @@ struct ScalePlan {
     int khf;           // first bin with f > fs/4 (isHighFreq)
     int wmax;          // longest window (samples)
     long long slot_base;  // first slot of this scale within an instance
+    long long win_base;   // first entry of this scale in the window tables
     float aG;          // sqrt(pi) / (s fs): Gaussian exponent per sample
     float Kc;          // 2 sqrt(2) / (s fs): single-channel energy factor
     float K1;          // sqrt(2) / (s fs): MMP1 energy factor
-    float pad_;
+    float aG2;         // aG sqrt(log2 e): Gaussian as exp2(-(d aG2)^2)
+    int eoff;          // offset of this scale's expFactor table (bins k < klo, then k > khi)
+    int pad_;
+};
+
+// Window geometry of one (scale, t): first sample, length, and the window
+// centre c = t0fixed * fs split into integer and fraction (src/gabor.cpp:279-286).
+struct WinGeom {
+    int iL, W, ci;
+    float cf;
 };
 
 struct DictPlan {

@@ -1,0 +1,417 @@
+// Refresh kernel: windowed pruned FFT + closed-form energies + slot maxima.
+//
+// One CTA takes a work unit: up to kUnitPoints complex FFT points of one
+// (instance, scale, residue group), i.e. a batch of consecutive t-windows.
+// The unit body is compiled per sub-FFT size L = 2^LOGL, so index math, padded
+// strides and the radix sequence are compile-time.  Per channel:
+//   (1) load: Gaussian-windowed FP32 residual samples packed two per complex
+//       point, folded and twisted into the residue's sub-sequence;
+//   (2) batched shared-memory Stockham FFT (fft.cuh);
+//   (3) spectrum: X[k] from Z[k] and Z[Nh-k] for kBinsPerTask consecutive q
+//       per thread, energy in closed form, max kept in registers, then over the
+//       lanes of the window.
+// Window geometry (iL, length, centre) comes from host tables computed in FP64
+// with the reference's expressions, so the device does no per-window FP64.
+// Included from kernels.cuh.
+#pragma once
+
+constexpr int kVPT = kUnitPoints / kUnitThreads;
+constexpr int kBufFloat2 = kUnitPoints + kUnitPoints / 16 + 16;
+constexpr int kAccBins = kUnitPoints + kMaxWindowsPerUnit;
+constexpr int kBinsPerTask = 8;  // consecutive q per thread in the spectrum stage
+
+// shared-memory layout of a refresh CTA
+struct RefreshSmem {
+    static constexpr size_t buf = 0;
+    static constexpr size_t win = buf + sizeof(float2) * kBufFloat2;          // int4 (iL, W, ci, cf bits)
+    static constexpr size_t hf = win + sizeof(int4) * kMaxWindowsPerUnit;     // float
+    static constexpr size_t key = hf + sizeof(float) * kMaxWindowsPerUnit;    // u64
+    static constexpr size_t acc = key + sizeof(unsigned long long) * kMaxWindowsPerUnit;
+};
+
+template <int MODE>
+constexpr size_t refresh_smem_bytes() {
+    return RefreshSmem::acc + (MODE == MODE_SINGLE ? 0 : sizeof(float) * kAccBins * (MODE == MODE_MMP1 ? 3 : 1));
+}
+
+// e^{i psi} with psi = 2 theta_kk = 2 pi (2 kk c / Nfft), c = ci + cf the
+// window centre in samples (the phase correction of src/gabor.cpp:296-298,
+// doubled): the exact integer part through the table (or sincospif of an
+// exact fraction), the fractional part through sincospif.
+__device__ __forceinline__ float2 centre_rot(unsigned kk, int ci, float cf, unsigned nf,
+                                             const float2* __restrict__ tw) {
+    const unsigned m = (unsigned)(((unsigned long long)(2u * kk) * (unsigned)ci) & (nf - 1u));
+    float2 a;
+    if (nf <= (unsigned)kTwN) {
+        const float2 t = __ldg(tw + m * ((unsigned)kTwN / nf));
+        a = make_float2(t.x, -t.y);
+    } else {
+        float s, c;
+        sincospif(2.0f * (float)m / (float)nf, &s, &c);
+        a = make_float2(c, s);
+    }
+    float s, c;
+    sincospif(2.0f * (2.0f * (float)kk * cf / (float)nf), &s, &c);
+    return cmul(a, make_float2(c, s));
+}
+
+// expFactor of a phase-dependent bin (k < klo or k > khi), src/gabor.cpp:51
+__device__ __forceinline__ float exp_factor_tab(int k, const ScalePlan& sp, const float* __restrict__ etab) {
+    return __ldg(etab + sp.eoff + (k < sp.klo ? k : sp.klo + (k - sp.khi - 1)));
+}
+
+// fs |v|^2 normReal^2 of one channel (GaborComputer::compute,
+// src/gabor.cpp:54-71) in closed form K |X|^4 / (|X|^2 + e Re(X^2 e^{i psi}));
+// rot = e^{i psi}.
+__device__ __forceinline__ float energy_phase(float2 X, float e, float2 rot, float Kc) {
+    const float p = X.x * X.x + X.y * X.y;
+    const float re = (X.x * X.x - X.y * X.y) * rot.x - 2.0f * X.x * X.y * rot.y;
+    const float D = p + e * re;
+    return (D > 0.0f && p > 0.0f) ? Kc * p * (p / D) : 0.0f;
+}
+
+// MMP1 closed form from P = sum |X_c|^2 and S = sum X_c^2 (constraint of
+// src/mmp.cpp:9-21 folded into the normalisation); low-frequency bins.
+__device__ __forceinline__ float energy_mmp1(float P, float2 S, bool phase, float e, float2 rot, float K1) {
+    const float as = sqrtf(S.x * S.x + S.y * S.y);
+    if (!phase) return K1 * (P + as);
+    if (as == 0.0f) return K1 * P / (1.0f + e);
+    const float re = S.x * rot.x - S.y * rot.y;
+    const float D = as + e * re;
+    return D > 0.0f ? K1 * (P + as) * (as / D) : 0.0f;
+}
+
+__device__ __forceinline__ void emit_candidate(const BatchDev& b, int inst, int j, int t, int k, float e) {
+    const int slot = atomicAdd(b.ctr + CTR_CBINS, 1);
+    if (slot < b.cbin_cap) {
+        const int li = atomicAdd(&b.state[inst].nbins, 1);
+        if (li < b.inst_bin_cap) {
+            CandBin cb;
+            cb.inst = inst;
+            cb.j = j;
+            cb.t = t;
+            cb.k = k;
+            cb.e32 = e;
+            cb.pad = 0;
+            cb.e64 = 0.0;
+            b.cbins[slot] = cb;
+            b.inst_bins[(long long)inst * b.inst_bin_cap + li] = slot;
+            return;
+        }
+    }
+    b.state[inst].err = ERR_CAND_OVERFLOW;
+}
+
+__device__ __forceinline__ unsigned long long umax64(unsigned long long a, unsigned long long b) {
+    return a > b ? a : b;
+}
+
+// What the spectrum stage does with a bin's final energy.
+template <bool COLLECT>
+struct BinSink {
+    const BatchDev& b;
+    int inst, j, t, tcount;
+    unsigned thr_bits;
+    unsigned long long best;
+    __device__ __forceinline__ void put(int k, float e) {
+        if (COLLECT) {
+            if (__float_as_uint(e) >= thr_bits) emit_candidate(b, inst, j, t, k, e);
+        } else {
+            if (b.dump) b.dump[(long long)k * tcount + t] = e;
+            best = umax64(best, pack_key(e, (unsigned)k));
+        }
+    }
+};
+
+template <int LOGL, int MODE, bool COLLECT>
+__device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem, int inst, int j, int g, int t_start,
+                                          int nwin, unsigned thr_bits) {
+    constexpr int L = 1 << LOGL;
+    constexpr int CH = L < kBinsPerTask ? L : kBinsPerTask;  // q values per task
+    constexpr int TPW = L / CH;                                // tasks per window
+    float2* buf = reinterpret_cast<float2*>(smem + RefreshSmem::buf);
+    int4* s_win = reinterpret_cast<int4*>(smem + RefreshSmem::win);
+    float* s_hf = reinterpret_cast<float*>(smem + RefreshSmem::hf);
+    unsigned long long* s_key = reinterpret_cast<unsigned long long*>(smem + RefreshSmem::key);
+    float* acc = reinterpret_cast<float*>(smem + RefreshSmem::acc);
+
+    const InstPlan ip = b.insts[inst];
+    const DictPlan dp = b.dicts[ip.dict];
+    const ScalePlan sp = b.scales[dp.scale0 + j];
+    const int M = sp.M, F = sp.F;
+    const int Nh = sp.nfft >> 1;
+    const unsigned nfu = (unsigned)sp.nfft;
+    const bool pair = g >= 2;
+    const int nf = pair ? 2 : 1;
+    const int nb = g == 0 ? L + 1 : (pair ? 2 * L : L);  // bins per window (accumulator stride)
+    const int r = g == 0 ? 0 : (g == 1 ? M / 2 : g - 1);
+    const int rho0 = r, rho1 = M - r;                       // residues of the group's FFTs
+    const int tid = threadIdx.x, T = blockDim.x;
+    const float2* __restrict__ tw = b.tw;
+    const float* __restrict__ etab = b.etab;
+    const float aG2 = sp.aG2, Kc = sp.Kc;
+
+    {
+        const long long w0 = sp.win_base + t_start;
+        for (int w = tid; w < nwin; w += T) {
+            s_win[w] = __ldg(b.wtab + w0 + w);
+            s_hf[w] = __ldg(b.whf + w0 + w);
+            s_key[w] = 0ull;
+        }
+    }
+    float2 wr0 = make_float2(1.f, 0.f), wr1 = make_float2(1.f, 0.f);  // W_Nfft^rho
+    if (g >= 1) {
+        float s0, c0;
+        sincospif(-2.0f * (float)rho0 / (float)sp.nfft, &s0, &c0);
+        wr0 = make_float2(c0, s0);
+        sincospif(-2.0f * (float)rho1 / (float)sp.nfft, &s0, &c0);
+        wr1 = make_float2(c0, s0);
+    }
+    if (MODE != MODE_SINGLE) {
+        for (int i = tid; i < nwin * nb * (MODE == MODE_MMP1 ? 3 : 1); i += T) acc[i] = 0.0f;
+    }
+    __syncthreads();
+
+    const int ntasks = nwin * TPW;
+    for (int c = 0; c < ip.C; ++c) {
+        const float* __restrict__ x = b.residual32 + ip.res_off + (long long)c * dp.N;
+        // (1) load: y_r[n'] = sum_m z[n' + mL] W_Nh^{r (n' + mL)}
+        for (int idx = tid; idx < (nwin << LOGL); idx += T) {
+            const int w = idx >> LOGL;
+            const int np = idx & (L - 1);
+            const int4 m = s_win[w];
+            const float cf = __int_as_float(m.w);
+            const float* __restrict__ xs = x + m.x;
+            float2 a1 = make_float2(0.f, 0.f), a2 = make_float2(0.f, 0.f);
+            int n = np;
+            for (int mm = 0; mm < F; ++mm, n += L) {
+                const int i0 = 2 * n;
+                if (i0 >= m.y) break;
+                const float x0 = __ldg(xs + i0);
+                const float x1 = (i0 + 1 < m.y) ? __ldg(xs + i0 + 1) : 0.0f;
+                const float d0 = (float)(i0 - m.z) - cf;
+                const float y0 = d0 * aG2, y1 = (d0 + 1.0f) * aG2;
+                const float2 z = make_float2(x0 * exp2f(-y0 * y0), x1 * exp2f(-y1 * y1));
+                if (g == 0) {
+                    a1 = cadd(a1, z);
+                } else if (g == 1) {
+                    // W_Nh^{(M/2) n} = W_{2L}^{n}
+                    a1 = cadd(a1, cmul(z, __ldg(tw + ((n & (2 * L - 1)) << (12 - LOGL)))));
+                } else {
+                    const unsigned rn = ((unsigned)r * (unsigned)n) & (unsigned)(Nh - 1);
+                    float2 t;
+                    if (Nh <= kTwN) {
+                        t = __ldg(tw + rn * (unsigned)(kTwN / Nh));
+                    } else {
+                        float s, cc;
+                        sincospif(-2.0f * (float)rn / (float)Nh, &s, &cc);
+                        t = make_float2(cc, s);
+                    }
+                    a1 = cadd(a1, cmul(z, t));
+                    a2 = cadd(a2, cmulc(z, t));
+                }
+            }
+            const int o = (w * nf) << LOGL;
+            buf[pad16(o + np)] = a1;
+            if (pair) buf[pad16(o + L + np)] = cmul(a2, __ldg(tw + (np << (13 - LOGL))));
+        }
+        __syncthreads();
+        // (2) FFT of every sub-sequence in the unit
+        fft_batch_t<kVPT, kTwN, LOGL>(buf, (nwin * nf) << LOGL, tw);
+        // (3) spectrum, energies, maxima
+        const bool last = (c == ip.C - 1);
+        for (int base = 0; base < ntasks; base += T) {
+            const int task = base + tid;
+            const bool valid = task < ntasks;
+            const int w = valid ? task / TPW : 0;
+            const int q0 = (task - w * TPW) * CH;
+            BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0ull};
+            if (valid) {
+                const int4 m = s_win[w];
+                const float cf = __int_as_float(m.w);
+                const int kmin = M * q0 + (pair ? min(rho0, rho1) : (g == 1 ? rho0 : 0));
+                const int kmax = (g == 0 && q0 == 0) ? Nh
+                                                     : M * (q0 + CH - 1) + (pair ? max(rho0, rho1) : (g == 1 ? rho0 : 0));
+                const bool phase = kmin < sp.klo || kmax > sp.khi;
+                float2 hrot = make_float2(1.f, 0.f), step = make_float2(1.f, 0.f);
+                if (phase) {
+                    float s, cc;
+                    sincospif(-2.0f * s_hf[w], &s, &cc);  // e^{-2 pi i fs t0} for high bins
+                    hrot = make_float2(cc, s);
+                    step = centre_rot((unsigned)M, m.z, cf, nfu, tw);  // psi increment from q to q + 1
+                }
+                const int o0 = (w * nf) << LOGL;
+                const int o1 = o0 + L;
+#pragma unroll 1
+                for (int h = 0; h < nf; ++h) {
+                    const int rho = h ? rho1 : rho0;
+                    const float2 wr = h ? wr1 : wr0;
+                    const int oa = h ? o1 : o0;                // A = Y_h[q]
+                    const int ob = pair ? (h ? o0 : o1) : o0;  // B = partner FFT
+                    float2 rot = make_float2(1.f, 0.f);
+                    if (phase) rot = centre_rot((unsigned)(M * q0 + rho), m.z, cf, nfu, tw);
+                    const int pa = pad16(oa + q0);
+#pragma unroll 2
+                    for (int qq = 0; qq < CH; ++qq) {
+                        const int q = q0 + qq;
+                        const int k = M * q + rho;
+                        const float2 A = buf[pa + qq];
+                        const int qb = (g == 0) ? ((L - q) & (L - 1)) : (L - 1 - q);
+                        const float2 Bq = buf[pad16(ob + qb)];
+                        const float2 t = __ldg(tw + (q << (12 - LOGL)));
+                        const float2 wk = (g == 0) ? t : cmul(wr, t);
+                        const float ex = 0.5f * (A.x + Bq.x), ey = 0.5f * (A.y - Bq.y);
+                        const float dx = 0.5f * (A.x - Bq.x), dy = 0.5f * (A.y + Bq.y);
+                        const float2 X = make_float2(ex + wk.x * dy + wk.y * dx, ey + wk.y * dy - wk.x * dx);
+                        if (k < sp.fcount) {
+                            const bool pk = phase && (k < sp.klo || k > sp.khi);
+                            const int ai = w * nb + q + h * L;
+                            if (MODE == MODE_SINGLE || MODE == MODE_MMP3 || k >= sp.khf) {
+                                float e;
+                                if (pk) e = energy_phase(X, exp_factor_tab(k, sp, etab),
+                                                         k >= sp.khf ? cmul(rot, hrot) : rot, Kc);
+                                else e = Kc * (X.x * X.x + X.y * X.y);
+                                if (MODE == MODE_SINGLE) sink.put(k, e);
+                                else acc[ai] += e;
+                            } else {
+                                acc[ai] += X.x * X.x + X.y * X.y;
+                                acc[nwin * nb + ai] += X.x * X.x - X.y * X.y;
+                                acc[2 * nwin * nb + ai] += 2.0f * X.x * X.y;
+                            }
+                        }
+                        if (phase) rot = cmul(rot, step);
+                    }
+                }
+                if (g == 0 && q0 == 0 && Nh < sp.fcount) {
+                    // Nyquist bin k = Nh (a high-frequency bin): X = Re Z[0] - Im Z[0]
+                    const float2 Z0 = buf[pad16(o0)];
+                    const float2 X = make_float2(Z0.x - Z0.y, 0.0f);
+                    const bool pk = Nh < sp.klo || Nh > sp.khi;
+                    const float e = pk ? energy_phase(X, exp_factor_tab(Nh, sp, etab),
+                                                      cmul(centre_rot((unsigned)Nh, m.z, cf, nfu, tw), hrot), Kc)
+                                       : Kc * X.x * X.x;
+                    if (MODE == MODE_SINGLE) sink.put(Nh, e);
+                    else acc[w * nb + L] += e;
+                }
+                if (MODE != MODE_SINGLE && last) {
+                    // energies of the accumulated channels
+                    const int nq = (g == 0 && q0 == 0) ? CH + 1 : CH;
+#pragma unroll 1
+                    for (int h = 0; h < nf; ++h) {
+                        const int rho = h ? rho1 : rho0;
+                        float2 rot = make_float2(1.f, 0.f);
+                        if (phase && MODE == MODE_MMP1) rot = centre_rot((unsigned)(M * q0 + rho), m.z, cf, nfu, tw);
+#pragma unroll 1
+                        for (int qq = 0; qq < nq; ++qq) {
+                            const bool nyq = qq == CH;
+                            const int q = nyq ? L : q0 + qq;
+                            const int k = nyq ? Nh : M * q + rho;
+                            if (k < sp.fcount && !(nyq && h == 1)) {
+                                const int ai = w * nb + q + h * L;
+                                float e;
+                                if (MODE == MODE_MMP3 || k >= sp.khf) {
+                                    e = acc[ai];
+                                } else {
+                                    const bool pk = k < sp.klo;
+                                    e = energy_mmp1(acc[ai], make_float2(acc[nwin * nb + ai], acc[2 * nwin * nb + ai]),
+                                                    pk, pk ? exp_factor_tab(k, sp, etab) : 0.0f, rot, sp.K1);
+                                }
+                                sink.put(k, e);
+                            }
+                            if (phase && MODE == MODE_MMP1 && !nyq) rot = cmul(rot, step);
+                        }
+                    }
+                }
+            }
+            if (!COLLECT && (MODE == MODE_SINGLE || last)) {
+                unsigned long long best = sink.best;
+                // max over the lanes of this window (TPW consecutive, aligned lanes)
+                if (TPW >= 32) {
+#pragma unroll
+                    for (int off = 16; off; off >>= 1) best = umax64(best, __shfl_xor_sync(0xffffffffu, best, off));
+                    if ((tid & 31) == 0 && valid) atomicMax(s_key + w, best);
+                } else {
+#pragma unroll
+                    for (int off = TPW / 2; off; off >>= 1) best = umax64(best, __shfl_xor_sync(0xffffffffu, best, off));
+                    if ((tid & (TPW - 1)) == 0 && valid) s_key[w] = best;
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    if (!COLLECT) {
+        unsigned long long* out = b.slots + ip.slot_off + sp.slot_base;
+        for (int w = tid; w < nwin; w += T) out[(long long)(t_start + w) * sp.G + g] = s_key[w];
+    }
+    __syncthreads();
+}
+
+// Out-of-line instance of one size, for the candidate path's runtime dispatch.
+template <int LOGL, int MODE>
+__device__ __noinline__ void collect_body(const BatchDev& b, unsigned char* smem, int inst, int j, int g, int t,
+                                          unsigned thr_bits) {
+    unit_body<LOGL, MODE, true>(b, smem, inst, j, g, t, 1, thr_bits);
+}
+
+#ifndef EMPI_REFRESH_MIN_BLOCKS
+#define EMPI_REFRESH_MIN_BLOCKS 1
+#endif
+
+// Refresh of one sub-FFT size: CTAs pull (instance, scale, group, t-batch)
+// units from that size's list, which the schedule filled.
+template <int MODE, int LOGL>
+__global__ void __launch_bounds__(kUnitThreads, EMPI_REFRESH_MIN_BLOCKS) k_refresh(BatchDev b) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_unit;
+    const int total = min(b.lcount[LOGL], b.lcap[LOGL]);
+    const int4* __restrict__ list = b.units + b.loff[LOGL];
+    for (;;) {
+        if (threadIdx.x == 0) s_unit = atomicAdd(b.lhead + LOGL, 1);
+        __syncthreads();
+        const int u = s_unit;
+        __syncthreads();
+        if (u >= total) break;
+        const int4 un = list[u];  // (instance, scale | group << 16, t_start, nwin)
+        unit_body<LOGL, MODE, false>(b, smem, un.x, un.y & 0xffff, un.y >> 16, un.z, un.w, 0u);
+    }
+}
+
+// FP32 recompute of the candidate slots (one window each), emitting every bin
+// within the band of the instance's best.
+template <int MODE>
+__global__ void __launch_bounds__(kUnitThreads, 1) k_collect(BatchDev b) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_unit;
+    const int total = min(b.ctr[CTR_CSLOTS], b.cslot_cap);
+    for (;;) {
+        if (threadIdx.x == 0) s_unit = atomicAdd(b.ctr + CTR_CSLOT_Q, 1);
+        __syncthreads();
+        const int u = s_unit;
+        __syncthreads();
+        if (u >= total) break;
+        const CandSlot cs = b.cslots[u];
+        const unsigned best = (unsigned)(b.state[cs.inst].best32 >> 32);
+        const unsigned thr = __float_as_uint(__uint_as_float(best) * (1.0f - b.band));
+        const InstPlan ip = b.insts[cs.inst];
+        switch (b.scales[b.dicts[ip.dict].scale0 + cs.j].logL) {
+#define EMPI_COLLECT_CASE(LG) \
+    case LG: collect_body<LG, MODE>(b, smem, cs.inst, cs.j, cs.g, cs.t, thr); break;
+            EMPI_COLLECT_CASE(0)
+            EMPI_COLLECT_CASE(1)
+            EMPI_COLLECT_CASE(2)
+            EMPI_COLLECT_CASE(3)
+            EMPI_COLLECT_CASE(4)
+            EMPI_COLLECT_CASE(5)
+            EMPI_COLLECT_CASE(6)
+            EMPI_COLLECT_CASE(7)
+            EMPI_COLLECT_CASE(8)
+            EMPI_COLLECT_CASE(9)
+            EMPI_COLLECT_CASE(10)
+            EMPI_COLLECT_CASE(11)
+            EMPI_COLLECT_CASE(12)
+#undef EMPI_COLLECT_CASE
+            default: break;
+        }
+    }
+}
