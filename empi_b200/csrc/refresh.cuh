@@ -355,7 +355,7 @@ __device__ __noinline__ void collect_body(const BatchDev& b, unsigned char* smem
 }
 
 #ifndef EMPI_REFRESH_MIN_BLOCKS
-#define EMPI_REFRESH_MIN_BLOCKS 1
+#define EMPI_REFRESH_MIN_BLOCKS 2
 #endif
 
 // Refresh of one sub-FFT size: CTAs pull (instance, scale, group, t-batch)
