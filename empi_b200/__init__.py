@@ -74,7 +74,7 @@ EXPORTS = [
     "empi_workspace_atom_count", "empi_workspace_subtract_atom", "empi_workspace_energy_map",
     "empi_subtract_atom_from_signal", "empi_batch_create", "empi_batch_destroy", "empi_batch_load",
     "empi_batch_run", "empi_batch_atoms", "empi_batch_total_energy", "empi_batch_get_stats",
-    "empi_decompose", "empi_run_config", "empi_book_write",
+    "empi_decompose", "empi_run_config", "empi_book_write", "empi_subtract_atom_from_signal_noalloc",
 ]
 
 _lib = None
@@ -112,6 +112,8 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.empi_workspace_subtract_atom.argtypes = [vp, dp, dp, ctypes.c_int]
     L.empi_workspace_energy_map.argtypes = [vp, ctypes.c_int, fp]
     L.empi_subtract_atom_from_signal.argtypes = [vp, dp, dp, ctypes.c_int, ctypes.c_double, ctypes.c_int]
+    L.empi_subtract_atom_from_signal_noalloc.argtypes = [ctypes.c_int, vp, dp, dp, ctypes.c_int, ctypes.c_double,
+                                                         ctypes.c_int]
     L.empi_batch_create.argtypes = [vp, ctypes.c_int, ctypes.POINTER(Dictionary), ctypes.POINTER(Settings),
                                     ctypes.POINTER(Epoch), ctypes.c_int, ctypes.POINTER(vp)]
     L.empi_batch_destroy.argtypes = [vp]

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1046,5 +1047,64 @@ extern "C" empi_status empi_subtract_atom_from_signal(empi_engine* eng, double* 
     CUDA_TRY(cudaMemcpyAsync(samples, x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaMemcpyAsync(params, p.p, sizeof(double) * 6, cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
+    return ok();
+}
+
+// ------------------------------------------------------------ allocation-free subtraction
+
+// Device copy of the signal (EMPI_NOALLOC_MAX_SAMPLES doubles) followed by the
+// six atom params, for empi_subtract_atom_from_signal_noalloc.  It is a fixed
+// static array so callers that may not allocate (stream capture, a device
+// owned by another memory pool) can still run the subtraction; every device
+// that loads the library holds these 8 MiB until exit.
+static __device__ __align__(256) double g_subtract_staging[EMPI_NOALLOC_MAX_SAMPLES + 8];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_staging_mutex;
+double* g_staging_ptr[kMaxDevices] = {};  // device address of the array, per device
+}  // namespace
+
+extern "C" empi_status empi_subtract_atom_from_signal_noalloc(int device, void* stream, double* params,
+                                                              double* samples, int n, double fs, int fit) {
+    if (!params || !samples || !(fs > 0)) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    if (n <= 0 || n > EMPI_NOALLOC_MAX_SAMPLES)
+        return fail(EMPI_ERR_INVALID_ARGUMENT, "signalLongerThanStaticScratch");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return fail(EMPI_ERR_NO_DEVICE, "noCudaDevice");
+    if (device < 0 || device >= count || device >= kMaxDevices) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidDevice");
+    int prev = 0;
+    CUDA_TRY(cudaGetDevice(&prev));
+    CUDA_TRY(cudaSetDevice(device));
+    double* base = nullptr;
+    {
+        // set-up once per device, with that device current: in host code the
+        // array's name is only a stand-in, the kernel needs its device address
+        std::lock_guard<std::mutex> lock(g_staging_mutex);
+        if (!g_staging_ptr[device]) {
+            double* p = nullptr;
+            cudaError_t ce = cudaGetSymbolAddress((void**)&p, g_subtract_staging);
+            if (ce != cudaSuccess || !p) {
+                cudaSetDevice(prev);
+                return fail(EMPI_ERR_CUDA, std::string("cuda: ") + cudaGetErrorString(ce) + " (staging address)");
+            }
+            g_staging_ptr[device] = p;
+        }
+        base = g_staging_ptr[device];
+    }
+    double* x = base;
+    double* prm = base + EMPI_NOALLOC_MAX_SAMPLES;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t ce = cudaMemcpyAsync(x, samples, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, s);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(prm, params, sizeof(double) * 6, cudaMemcpyHostToDevice, s);
+    if (ce == cudaSuccess) {
+        k_subtract_signal<<<1, 256, 0, s>>>(x, nullptr, n, fs, prm, fit);
+        ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(samples, x, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(params, prm, sizeof(double) * 6, cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    cudaSetDevice(prev);
+    if (ce != cudaSuccess) return fail(EMPI_ERR_CUDA, std::string("cuda: ") + cudaGetErrorString(ce));
     return ok();
 }

@@ -131,6 +131,22 @@ empi_status empi_workspace_energy_map(empi_workspace* ws, int scale, float* ener
 empi_status empi_subtract_atom_from_signal(empi_engine* engine, double* params, double* samples,
                                            int n, double fs, int fit);
 
+/* Same as empi_subtract_atom_from_signal, for callers that cannot allocate
+ * device memory: code running inside CUDA stream capture, or next to a
+ * framework whose memory pool owns the device (cudaMalloc and cudaFree are
+ * not allowed in the first case and also synchronise the whole device).  No
+ * counterpart in the reference: the device copy of the signal and params
+ * lives in a fixed static device array instead of per-call allocations, so
+ * n may not exceed EMPI_NOALLOC_MAX_SAMPLES (8 MiB of doubles per device,
+ * held from library load until exit).  `stream` is a cudaStream_t (NULL =
+ * the default stream).  The first call on a device looks the array up and
+ * should happen before any stream capture.  All calls on a device share the
+ * array, so calls that overlap on the GPU (other threads, other streams)
+ * race and must be serialised by the caller. */
+#define EMPI_NOALLOC_MAX_SAMPLES (1 << 20)
+empi_status empi_subtract_atom_from_signal_noalloc(int device, void* stream, double* params,
+                                                   double* samples, int n, double fs, int fit);
+
 /* ------------------------------------------------ batched decomposition */
 
 /* DecompositionSettings, inc/classes.hpp:84-87 */
