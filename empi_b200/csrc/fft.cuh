@@ -153,4 +153,12 @@ __device__ __forceinline__ void fft_batch_t(float2* buf, int points, const float
     for (int logNs = first; logNs < LOGL; logNs += 4) fft_pass<16, VPT, TW_N>(buf, LOGL, logNs, points, tw);
 }
 
+// The radix-16 passes that follow an odd first pass done by the caller.
+template <int VPT, int TW_N, int LOGL>
+__device__ __forceinline__ void fft_batch_rest(float2* buf, int points, const float2* __restrict__ tw) {
+    constexpr int first = LOGL & 3;
+#pragma unroll
+    for (int logNs = first; logNs < LOGL; logNs += 4) fft_pass<16, VPT, TW_N>(buf, LOGL, logNs, points, tw);
+}
+
 }  // namespace empi

@@ -268,15 +268,15 @@ __global__ void k_sched_a(BatchDev b, int mode, int only_scale, double tA_in, do
             c0 = (int)(s0 / kChunk);
             nc = (int)(s1 / kChunk) - c0 + 1;
             // statistics: reference-equivalent FFT flops (2.5 Nfft log2 Nfft per
-            // window and channel) and compulsory bytes (the residual span read
-            // once per channel, one 8-byte slot write per (window, group))
+            // window and channel) and compulsory bytes (the FP32 residual span
+            // read once per channel, one 8-byte slot write per (window, group))
             int iL0, iR0, iL1, iR1;
             double tf;
             window_bounds(grid_t(lo, dp.tMax, sp.tcount), sp.hw, dp.fs, dp.N, iL0, iR0, tf);
             window_bounds(grid_t(hi, dp.tMax, sp.tcount), sp.hw, dp.fs, dp.N, iL1, iR1, tf);
             const double lg = log2((double)sp.nfft);
             atomicAdd(b.stats + 0, (double)n * ip.C * 2.5 * sp.nfft * lg);
-            atomicAdd(b.stats + 1, 8.0 * ip.C * (double)(iR1 - iL0 + 1) + 8.0 * (double)n * sp.G);
+            atomicAdd(b.stats + 1, 4.0 * ip.C * (double)(iR1 - iL0 + 1) + 8.0 * (double)n * sp.G);
             atomicAdd(b.stats + 2, (double)n * sp.G);
         }
         units[j + 1] = nu;

@@ -175,14 +175,12 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
     const int ntasks = nwin * TPW;
     for (int c = 0; c < ip.C; ++c) {
         const float* __restrict__ x = b.residual32 + ip.res_off + (long long)c * dp.N;
-        // (1) load: y_r[n'] = sum_m z[n' + mL] W_Nh^{r (n' + mL)}
-        for (int idx = tid; idx < (nwin << LOGL); idx += T) {
-            const int w = idx >> LOGL;
-            const int np = idx & (L - 1);
-            const int4 m = s_win[w];
-            const float cf = __int_as_float(m.w);
+        // (1) load: y_r[n'] = sum_m z[n' + mL] W_Nh^{r (n' + mL)}; for the second
+        // FFT of a pair the sum is conjugate-twisted and multiplied by W_L^{n'}
+        auto load_point = [&](const int4& m, float cf, int np, float2& a1, float2& a2) {
             const float* __restrict__ xs = x + m.x;
-            float2 a1 = make_float2(0.f, 0.f), a2 = make_float2(0.f, 0.f);
+            a1 = make_float2(0.f, 0.f);
+            a2 = make_float2(0.f, 0.f);
             int n = np;
             for (int mm = 0; mm < F; ++mm, n += L) {
                 const int i0 = 2 * n;
@@ -203,21 +201,56 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     if (Nh <= kTwN) {
                         t = __ldg(tw + rn * (unsigned)(kTwN / Nh));
                     } else {
-                        float s, cc;
-                        sincospif(-2.0f * (float)rn / (float)Nh, &s, &cc);
-                        t = make_float2(cc, s);
+                        float sn, cs;
+                        sincospif(-2.0f * (float)rn / (float)Nh, &sn, &cs);
+                        t = make_float2(cs, sn);
                     }
                     a1 = cadd(a1, cmul(z, t));
                     a2 = cadd(a2, cmulc(z, t));
                 }
             }
-            const int o = (w * nf) << LOGL;
-            buf[pad16(o + np)] = a1;
-            if (pair) buf[pad16(o + L + np)] = cmul(a2, __ldg(tw + (np << (13 - LOGL))));
+            if (pair) a2 = cmul(a2, __ldg(tw + (np << (13 - LOGL))));
+        };
+        constexpr int FIRST = LOGL & 3;  // log2 of the odd first radix; 0: radix-16 passes only
+        if constexpr (FIRST != 0) {
+            // the first Stockham pass (radix 2^FIRST, no twiddles) fused into the load
+            constexpr int R0 = 1 << FIRST;
+            constexpr int LQ = LOGL - FIRST;  // log2 of L / R0
+            for (int job = tid; job < (nwin << LQ); job += T) {
+                const int w = job >> LQ;
+                const int jq = job & ((1 << LQ) - 1);
+                const int4 m = s_win[w];
+                const float cf = __int_as_float(m.w);
+                float2 v1[R0], v2[R0];
+#pragma unroll
+                for (int rr = 0; rr < R0; ++rr) load_point(m, cf, jq + (rr << LQ), v1[rr], v2[rr]);
+                const int o = ((w * nf) << LOGL) + jq * R0;
+                dft<R0>(v1);
+#pragma unroll
+                for (int rr = 0; rr < R0; ++rr) buf[pad16(o + rr)] = v1[rr];
+                if (pair) {
+                    dft<R0>(v2);
+#pragma unroll
+                    for (int rr = 0; rr < R0; ++rr) buf[pad16(o + L + rr)] = v2[rr];
+                }
+            }
+            __syncthreads();
+            fft_batch_rest<kVPT, kTwN, LOGL>(buf, (nwin * nf) << LOGL, tw);
+        } else {
+            for (int idx = tid; idx < (nwin << LOGL); idx += T) {
+                const int w = idx >> LOGL;
+                const int np = idx & (L - 1);
+                const int4 m = s_win[w];
+                float2 a1, a2;
+                load_point(m, __int_as_float(m.w), np, a1, a2);
+                const int o = (w * nf) << LOGL;
+                buf[pad16(o + np)] = a1;
+                if (pair) buf[pad16(o + L + np)] = a2;
+            }
+            __syncthreads();
+            // (2) FFT of every sub-sequence in the unit
+            fft_batch_t<kVPT, kTwN, LOGL>(buf, (nwin * nf) << LOGL, tw);
         }
-        __syncthreads();
-        // (2) FFT of every sub-sequence in the unit
-        fft_batch_t<kVPT, kTwN, LOGL>(buf, (nwin * nf) << LOGL, tw);
         // (3) spectrum, energies, maxima
         const bool last = (c == ip.C - 1);
         for (int base = 0; base < ntasks; base += T) {
