@@ -10,6 +10,10 @@ Writes:
   smp0.b          the reference CLI's book for workload 0 (SMP 1x1280 @128 Hz)
   smp0.cfg        the config that produced it (signal: smp0.bin, regenerated
                   from the seed by the tests)
+  scale_cases.json  larger cases at BASELINE shapes (the bench workload's first
+                  epoch, 16384-sample windows that need folded transforms,
+                  energyError 0.001 with Nfft up to 2^17), with the
+                  restatement's best-to-second margins for the tie rule
 """
 from __future__ import annotations
 
@@ -49,7 +53,39 @@ def case_signal(wl, ov):
     return w.fs, w.epochs[0]
 
 
+SCALE_CASES = [
+    ("mmp2_bench_epoch0", "mmp2", 1, {"epochs": 1}, 0.01, 15, 99.0, {}),
+    ("mmp3_2x8192_512", "mmp3", 2, {"epochs": 1, "channels": 2, "samples": 8192}, 0.005, 6, 100.0, {}),
+    ("smp_16384_512_fold", "smp", 2, {"epochs": 1, "channels": 1, "samples": 16384}, 0.005, 4, 100.0, {}),
+    ("smp_2048_128_eps001", "smp", 0, {"samples": 2048, "seed": 44}, 0.001, 5, 100.0, {}),
+]
+
+
+def scale_main():
+    out = []
+    for name, variant, wl, ov, eps, iters, pct, lim in SCALE_CASES:
+        fs, x = case_signal(wl, ov)
+        xs = x.T.astype(np.float64)
+        kw = dict(smin=lim.get("smin", 0.0), smax=lim.get("smax", math.inf), fmax=lim.get("fmax", math.inf))
+        r = O.ref_decompose(variant, fs, xs, eps, iters, pct, **kw)
+        m = O.decompose(variant, fs, xs, eps, iters, pct, **kw)
+        rec = {"name": name, "variant": variant, "workload": wl, "overrides": ov, "fs": fs, "energy_error": eps,
+               "iterations": iters, "energy_percent": pct, "limits": lim, "channels": int(x.shape[1]),
+               "samples": int(x.shape[0]),
+               "signal_sha_f32": __import__("hashlib").sha256(x.tobytes()).hexdigest(),
+               "counts": [int(v) for v in r.natoms],
+               "atoms": [[list(map(float, r.atoms[c, a])) for a in range(r.natoms[c])] for c in range(xs.shape[0])],
+               "energies": [[None if not np.isfinite(v) else float(v) for v in row] for row in r.energies],
+               "margins": [[None if not np.isfinite(v) else float(v) for v in row] for row in m.margins]}
+        out.append(rec)
+        print(name, rec["counts"], flush=True)
+    with open(os.path.join(HERE, "scale_cases.json"), "w") as f:
+        json.dump({"cases": out}, f, indent=1)
+
+
 def main():
+    if "--scale" in sys.argv:
+        return scale_main()
     if not O.ref_available():
         raise SystemExit("oracle/_ref/libempiref.so missing: run `make -C oracle ref` first")
     out = []
