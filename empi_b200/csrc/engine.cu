@@ -131,13 +131,17 @@ extern "C" empi_status empi_engine_create(const empi_engine_opts* opts, empi_eng
         CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
         e->own_stream = true;
     }
-    std::vector<float2> tw(kTwN);
+    // coarse table W_kTwN^m, then fine table W_(2^26)^m (twiddle_pow2)
+    std::vector<float2> tw(2 * kTwN);
     for (int m = 0; m < kTwN; ++m) {
-        long double a = 6.283185307179586476925286766559005768L * (long double)m / (long double)kTwN;
+        const long double two_pi = 6.283185307179586476925286766559005768L;
+        const long double a = two_pi * (long double)m / (long double)kTwN;
+        const long double af = two_pi * (long double)m / (long double)(1ll << kTwFineLog);
         tw[m] = make_float2((float)cosl(a), (float)(-sinl(a)));
+        tw[kTwN + m] = make_float2((float)cosl(af), (float)(-sinl(af)));
     }
-    CUDA_TRY(cudaMalloc(&e->tw, sizeof(float2) * kTwN));
-    CUDA_TRY(cudaMemcpy(e->tw, tw.data(), sizeof(float2) * kTwN, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMalloc(&e->tw, sizeof(float2) * 2 * kTwN));
+    CUDA_TRY(cudaMemcpy(e->tw, tw.data(), sizeof(float2) * 2 * kTwN, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
     for (int i = 0; i < kSizes; ++i) {
         CUDA_TRY(cudaStreamCreateWithFlags(&e->aux[i], cudaStreamNonBlocking));

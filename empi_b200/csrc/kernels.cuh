@@ -74,7 +74,7 @@ struct BatchDev {
     const DictPlan* dicts;
     const InstPlan* insts;
     const int2* blk_ic;   // (instance, channel) of each per-channel block
-    const float2* tw;     // exp(-2 pi i m / kTwN)
+    const float2* tw;     // exp(-2 pi i m / kTwN), then exp(-2 pi i m / 2^26), m < kTwN
     const float* input;   // all epochs, float32 interleaved
     int ninst, nblk_ic, cmax, iter_max, mode;
     double residual_energy;
@@ -175,11 +175,21 @@ __device__ __forceinline__ int upper_index(const int* prefix, int n, int u) {
     return lo;
 }
 
-// exp(-2 pi i a / b) for integers a < b (b a power of two)
-__device__ __forceinline__ float2 twiddle_frac(long long a, long long b, const float2* tw) {
-    if (b <= kTwN) return __ldg(tw + a * (kTwN / b));
+// exp(-2 pi i m / n) for n a power of two and m < n.  The twiddle buffer holds
+// the coarse table W_kTwN^i followed by the fine table W_(2^26)^i (i < kTwN),
+// both rounded from exact values on the host.  n <= kTwN: one coarse entry;
+// n <= 2^26: W_kTwN^(m >> sh) * W_n^(m mod 2^sh) with sh = log2 n - 13, the
+// second factor a fine entry; larger n: sincospif.
+__device__ __forceinline__ float2 twiddle_pow2(unsigned m, unsigned n, const float2* __restrict__ tw) {
+    if (n <= (unsigned)kTwN) return __ldg(tw + m * ((unsigned)kTwN / n));
+    if (n <= (1u << kTwFineLog)) {
+        const int sh = 31 - __clz(n) - kTwLog;
+        const float2 hi = __ldg(tw + (m >> sh));
+        const float2 lo = __ldg(tw + kTwN + ((m & ((1u << sh) - 1u)) << (kTwFineLog - kTwLog - sh)));
+        return cmul(hi, lo);
+    }
     float s, c;
-    sincospif(-2.0f * (float)a / (float)b, &s, &c);
+    sincospif(-2.0f * (float)m / (float)n, &s, &c);
     return make_float2(c, s);
 }
 

@@ -25,6 +25,8 @@ namespace empi {
 
 constexpr int kChunk = 1024;          // slots per tournament-tree leaf chunk
 constexpr int kTwN = 8192;            // length of the FP32 twiddle table
+constexpr int kTwLog = 13;            // log2 kTwN
+constexpr int kTwFineLog = 26;        // the fine table holds W_2^26^i, i < kTwN
 constexpr int kUnitPoints = 8192;     // complex points per CTA work unit
 constexpr int kUnitThreads = 512;     // threads per refresh CTA
 constexpr int kMaxWindowsPerUnit = 1024;

@@ -25,8 +25,8 @@ struct RefreshSmem {
     static constexpr size_t buf = 0;
     static constexpr size_t win = buf + sizeof(float2) * kBufFloat2;          // int4 (iL, W, ci, cf bits)
     static constexpr size_t hf = win + sizeof(int4) * kMaxWindowsPerUnit;     // float
-    static constexpr size_t key = hf + sizeof(float) * kMaxWindowsPerUnit;    // u64
-    static constexpr size_t acc = key + sizeof(unsigned long long) * kMaxWindowsPerUnit;
+    static constexpr size_t key = hf + sizeof(float) * kMaxWindowsPerUnit;    // u32 energy bits
+    static constexpr size_t acc = key + sizeof(unsigned) * kMaxWindowsPerUnit;
 };
 
 template <int MODE>
@@ -41,15 +41,8 @@ constexpr size_t refresh_smem_bytes() {
 __device__ __forceinline__ float2 centre_rot(unsigned kk, int ci, float cf, unsigned nf,
                                              const float2* __restrict__ tw) {
     const unsigned m = (unsigned)(((unsigned long long)(2u * kk) * (unsigned)ci) & (nf - 1u));
-    float2 a;
-    if (nf <= (unsigned)kTwN) {
-        const float2 t = __ldg(tw + m * ((unsigned)kTwN / nf));
-        a = make_float2(t.x, -t.y);
-    } else {
-        float s, c;
-        sincospif(2.0f * (float)m / (float)nf, &s, &c);
-        a = make_float2(c, s);
-    }
+    const float2 t = twiddle_pow2(m, nf, tw);
+    const float2 a = make_float2(t.x, -t.y);
     float s, c;
     sincospif(2.0f * (2.0f * (float)kk * cf / (float)nf), &s, &c);
     return cmul(a, make_float2(c, s));
@@ -102,23 +95,21 @@ __device__ __forceinline__ void emit_candidate(const BatchDev& b, int inst, int 
     b.state[inst].err = ERR_CAND_OVERFLOW;
 }
 
-__device__ __forceinline__ unsigned long long umax64(unsigned long long a, unsigned long long b) {
-    return a > b ? a : b;
-}
-
-// What the spectrum stage does with a bin's final energy.
+// What the spectrum stage does with a bin's final energy.  The slot keeps only
+// its maximum energy (the tree keys slots by index); negative, NaN and
+// infinite energies count as 0, as in pack_key.
 template <bool COLLECT>
 struct BinSink {
     const BatchDev& b;
     int inst, j, t, tcount;
     unsigned thr_bits;
-    unsigned long long best;
+    float best;
     __device__ __forceinline__ void put(int k, float e) {
         if (COLLECT) {
             if (__float_as_uint(e) >= thr_bits) emit_candidate(b, inst, j, t, k, e);
         } else {
             if (b.dump) b.dump[(long long)k * tcount + t] = e;
-            best = umax64(best, pack_key(e, (unsigned)k));
+            best = fmaxf(best, e <= 3.0e38f ? e : 0.0f);
         }
     }
 };
@@ -132,7 +123,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
     float2* buf = reinterpret_cast<float2*>(smem + RefreshSmem::buf);
     int4* s_win = reinterpret_cast<int4*>(smem + RefreshSmem::win);
     float* s_hf = reinterpret_cast<float*>(smem + RefreshSmem::hf);
-    unsigned long long* s_key = reinterpret_cast<unsigned long long*>(smem + RefreshSmem::key);
+    unsigned* s_key = reinterpret_cast<unsigned*>(smem + RefreshSmem::key);
     float* acc = reinterpret_cast<float*>(smem + RefreshSmem::acc);
 
     const InstPlan ip = b.insts[inst];
@@ -156,7 +147,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
         for (int w = tid; w < nwin; w += T) {
             s_win[w] = __ldg(b.wtab + w0 + w);
             s_hf[w] = __ldg(b.whf + w0 + w);
-            s_key[w] = 0ull;
+            s_key[w] = 0u;
         }
     }
     float2 wr0 = make_float2(1.f, 0.f), wr1 = make_float2(1.f, 0.f);  // W_Nfft^rho
@@ -197,14 +188,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     a1 = cadd(a1, cmul(z, __ldg(tw + ((n & (2 * L - 1)) << (12 - LOGL)))));
                 } else {
                     const unsigned rn = ((unsigned)r * (unsigned)n) & (unsigned)(Nh - 1);
-                    float2 t;
-                    if (Nh <= kTwN) {
-                        t = __ldg(tw + rn * (unsigned)(kTwN / Nh));
-                    } else {
-                        float sn, cs;
-                        sincospif(-2.0f * (float)rn / (float)Nh, &sn, &cs);
-                        t = make_float2(cs, sn);
-                    }
+                    const float2 t = twiddle_pow2(rn, (unsigned)Nh, tw);
                     a1 = cadd(a1, cmul(z, t));
                     a2 = cadd(a2, cmulc(z, t));
                 }
@@ -258,7 +242,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
             const bool valid = task < ntasks;
             const int w = valid ? task / TPW : 0;
             const int q0 = (task - w * TPW) * CH;
-            BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0ull};
+            BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
             if (valid) {
                 const int4 m = s_win[w];
                 const float cf = __int_as_float(m.w);
@@ -357,15 +341,15 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                 }
             }
             if (!COLLECT && (MODE == MODE_SINGLE || last)) {
-                unsigned long long best = sink.best;
-                // max over the lanes of this window (TPW consecutive, aligned lanes)
+                // max over the lanes of this window (TPW consecutive, aligned lanes);
+                // non-negative floats order as their bit patterns
+                unsigned best = __float_as_uint(sink.best);
                 if (TPW >= 32) {
-#pragma unroll
-                    for (int off = 16; off; off >>= 1) best = umax64(best, __shfl_xor_sync(0xffffffffu, best, off));
+                    best = __reduce_max_sync(0xffffffffu, best);
                     if ((tid & 31) == 0 && valid) atomicMax(s_key + w, best);
                 } else {
 #pragma unroll
-                    for (int off = TPW / 2; off; off >>= 1) best = umax64(best, __shfl_xor_sync(0xffffffffu, best, off));
+                    for (int off = TPW / 2; off; off >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, off));
                     if ((tid & (TPW - 1)) == 0 && valid) s_key[w] = best;
                 }
             }
@@ -375,7 +359,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
 
     if (!COLLECT) {
         unsigned long long* out = b.slots + ip.slot_off + sp.slot_base;
-        for (int w = tid; w < nwin; w += T) out[(long long)(t_start + w) * sp.G + g] = s_key[w];
+        for (int w = tid; w < nwin; w += T) out[(long long)(t_start + w) * sp.G + g] = (unsigned long long)s_key[w] << 32;
     }
     __syncthreads();
 }
