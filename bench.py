@@ -44,7 +44,9 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     # small cases for profiling runs (not bench numbers)
-    p.add_argument("--epochs", type=int, default=0, help="decompose only the first E epochs")
+    p.add_argument("--workload", type=int, default=WORKLOAD,
+                   help="synthetic workload index (empi_b200.synth); the default is the headline one")
+    p.add_argument("--epochs", type=int, default=0, help="decompose only the first E epochs (instances)")
     p.add_argument("--iterations", type=int, default=0, help="override the iteration count")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-roofline", action="store_true")
@@ -96,7 +98,7 @@ def reference_arm(args):
         return
     from empi_b200 import synth
 
-    w = synth.workload(WORKLOAD)
+    w = synth.workload(args.workload, epochs=args.epochs or None, iterations=args.iterations or None)
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
         r = run_reference(w, 5, threads)
@@ -126,7 +128,12 @@ def reference_arm(args):
 
 
 def workload_config(w, world):
-    return {"workload": f"{w.variant.upper()} {w.channels}ch x {len(w.epochs)} epochs x {w.samples} "
+    if len({e.shape for e in w.epochs}) > 1:
+        shape = (f"{len(w.epochs)} uneven instances ({sum(e.shape[1] for e in w.epochs)} channels, "
+                 f"{min(e.shape[0] for e in w.epochs)}-{max(e.shape[0] for e in w.epochs)} samples)")
+    else:
+        shape = f"{w.channels}ch x {len(w.epochs)} epochs x {w.samples}"
+    return {"workload": f"{w.variant.upper()} {shape} "
                         f"float32 @ {w.fs:g} Hz, energyError {w.energy_error}, {w.iterations} iterations, "
                         f"energyPercent {w.energy_percent}",
             "variant": w.variant, "channels": w.channels, "epochs": len(w.epochs), "samples": w.samples,
@@ -229,7 +236,7 @@ def ours(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-    w = synth.workload(WORKLOAD, seed=1000 + WORKLOAD + 7919 * rank, epochs=args.epochs or None,
+    w = synth.workload(args.workload, seed=1000 + args.workload + 7919 * rank, epochs=args.epochs or None,
                        iterations=args.iterations or None)
     stream = torch.cuda.Stream()
     eng = empi_b200.Engine(device=local, stream=stream.cuda_stream)
