@@ -20,6 +20,28 @@ constexpr int kBufFloat2 = kUnitPoints + kUnitPoints / 16 + 16;
 constexpr int kAccBins = kUnitPoints + kMaxWindowsPerUnit;
 constexpr int kBinsPerTask = 8;  // consecutive q per thread in the spectrum stage
 
+// W_2L = exp(-i pi / L) for L = 2^0 .. 2^13 (cos and -sin of pi / L, rounded to
+// float): the step of the spectrum stage's twiddle W_2L^q from bin q to q + 1.
+struct Rot {
+    float x, y;
+};
+constexpr Rot kW2L[14] = {
+    {-1.0f, 0.0f},
+    {0.0f, -1.0f},
+    {0.70710678118654752f, -0.70710678118654752f},
+    {0.92387953251128674f, -0.38268343236508977f},
+    {0.98078528040323043f, -0.19509032201612825f},
+    {0.99518472667219689f, -0.098017140329560602f},
+    {0.99879545620517241f, -0.049067674327418015f},
+    {0.99969881869620425f, -0.024541228522912288f},
+    {0.99992470183914454f, -0.012271538285719925f},
+    {0.99998117528260111f, -0.0061358846491544753f},
+    {0.99999529380957619f, -0.0030679567629659761f},
+    {0.99999882345170188f, -0.0015339801862847656f},
+    {0.99999970586288223f, -0.00076699031874270449f},
+    {0.99999992646571785f, -0.00038349518757139556f},
+};
+
 // shared-memory layout of a refresh CTA
 struct RefreshSmem {
     static constexpr size_t buf = 0;
@@ -114,6 +136,22 @@ struct BinSink {
     }
 };
 
+// Max of one window's bins over the lanes holding its tasks (TPW consecutive,
+// aligned lanes) into the window's shared key; non-negative floats order as
+// their bit patterns.
+template <int TPW>
+__device__ __forceinline__ void sink_reduce(float bestf, unsigned* s_key, int w, bool valid, int tid) {
+    unsigned best = __float_as_uint(bestf);
+    if (TPW >= 32) {
+        best = __reduce_max_sync(0xffffffffu, best);
+        if ((tid & 31) == 0 && valid) atomicMax(s_key + w, best);
+    } else {
+#pragma unroll
+        for (int off = TPW / 2; off; off >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, off));
+        if ((tid & (TPW - 1)) == 0 && valid) atomicMax(s_key + w, best);
+    }
+}
+
 template <int LOGL, int MODE, bool COLLECT>
 __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem, int inst, int j, int g, int t_start,
                                           int nwin, unsigned thr_bits) {
@@ -164,6 +202,31 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
     __syncthreads();
 
     const int ntasks = nwin * TPW;
+    // tasks with phase-dependent bins: tau < tlo (kmin < klo) and tau >= thi
+    // (kmax > khi); kmin and kmax grow with tau, so both ends are found by
+    // bisection (the q0 = 0 task of group 0, which also holds the Nyquist
+    // bin, has kmin = 0 < klo)
+    int tlo = 0, thi = TPW;
+    {
+        const int rmin = pair ? min(rho0, rho1) : (g == 1 ? rho0 : 0);
+        const int rmax = pair ? max(rho0, rho1) : (g == 1 ? rho0 : 0);
+        int lo = 0, hi = TPW;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (M * mid * CH + rmin >= sp.klo) hi = mid;
+            else lo = mid + 1;
+        }
+        tlo = lo;
+        lo = 0;
+        hi = TPW;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (M * (mid * CH + CH - 1) + rmax > sp.khi) hi = mid;
+            else lo = mid + 1;
+        }
+        thi = max(lo, tlo);
+    }
+    const int nph = tlo + (TPW - thi);
     for (int c = 0; c < ip.C; ++c) {
         const float* __restrict__ x = b.residual32 + ip.res_off + (long long)c * dp.N;
         // (1) load: y_r[n'] = sum_m z[n' + mL] W_Nh^{r (n' + mL)}; for the second
@@ -237,66 +300,225 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
         }
         // (3) spectrum, energies, maxima
         const bool last = (c == ip.C - 1);
-        for (int base = 0; base < ntasks; base += T) {
-            const int task = base + tid;
-            const bool valid = task < ntasks;
-            const int w = valid ? task / TPW : 0;
-            const int q0 = (task - w * TPW) * CH;
-            BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
-            if (valid) {
+        // Two passes (3a, 3b) for 64 <= L <= 2048.  Small transforms (L <= 32)
+        // are almost all phase-dependent bins; at L = 4096 a unit holds one or two
+        // windows, too few phase tasks to spread, and the single pass measured
+        // faster; MMP1 folds the phase into its channel sums.  Those keep the
+        // single pass.
+        constexpr bool kSplit = MODE != MODE_MMP1 && LOGL >= 6 && LOGL <= 11;
+        if constexpr (!kSplit) {
+            for (int base = 0; base < ntasks; base += T) {
+                const int task = base + tid;
+                const bool valid = task < ntasks;
+                const int w = valid ? task / TPW : 0;
+                const int q0 = (task - w * TPW) * CH;
+                BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
+                if (valid) {
+                    const int4 m = s_win[w];
+                    const float cf = __int_as_float(m.w);
+                    const int kmin = M * q0 + (pair ? min(rho0, rho1) : (g == 1 ? rho0 : 0));
+                    const int kmax = (g == 0 && q0 == 0) ? Nh
+                                                         : M * (q0 + CH - 1) + (pair ? max(rho0, rho1) : (g == 1 ? rho0 : 0));
+                    const bool phase = kmin < sp.klo || kmax > sp.khi;
+                    float2 hrot = make_float2(1.f, 0.f), step = make_float2(1.f, 0.f);
+                    if (phase) {
+                        float s, cc;
+                        sincospif(-2.0f * s_hf[w], &s, &cc);  // e^{-2 pi i fs t0} for high bins
+                        hrot = make_float2(cc, s);
+                        step = centre_rot((unsigned)M, m.z, cf, nfu, tw);  // psi increment from q to q + 1
+                    }
+                    const int o0 = (w * nf) << LOGL;
+                    const int o1 = o0 + L;
+    #pragma unroll 1
+                    for (int h = 0; h < nf; ++h) {
+                        const int rho = h ? rho1 : rho0;
+                        const float2 wr = h ? wr1 : wr0;
+                        const int oa = h ? o1 : o0;                // A = Y_h[q]
+                        const int ob = pair ? (h ? o0 : o1) : o0;  // B = partner FFT
+                        float2 rot = make_float2(1.f, 0.f);
+                        if (phase) rot = centre_rot((unsigned)(M * q0 + rho), m.z, cf, nfu, tw);
+                        const int pa = pad16(oa + q0);
+                        // partner L - 1 - q for g >= 1: a descending run inside one
+                        // 16-block, since (L - 1 - q0) mod 16 is 15 or 7
+                        const int pb = pad16(ob + L - 1 - q0);
+                        // W_2L^q: the table entry at q0, then one rotation by W_2L per bin
+                        float2 t = __ldg(tw + (q0 << (12 - LOGL)));
+    #pragma unroll 2
+                        for (int qq = 0; qq < CH; ++qq) {
+                            const int q = q0 + qq;
+                            const int k = M * q + rho;
+                            const float2 A = buf[pa + qq];
+                            const float2 Bq = (g == 0) ? buf[pad16(ob + ((L - q) & (L - 1)))] : buf[pb - qq];
+                            const float2 wk = (g == 0) ? t : cmul(wr, t);
+                            t = cmul(t, make_float2(kW2L[LOGL].x, kW2L[LOGL].y));
+                            const float ex = 0.5f * (A.x + Bq.x), ey = 0.5f * (A.y - Bq.y);
+                            const float dx = 0.5f * (A.x - Bq.x), dy = 0.5f * (A.y + Bq.y);
+                            const float2 X = make_float2(ex + wk.x * dy + wk.y * dx, ey + wk.y * dy - wk.x * dx);
+                            if (k < sp.fcount) {
+                                const bool pk = phase && (k < sp.klo || k > sp.khi);
+                                const int ai = w * nb + q + h * L;
+                                if (MODE == MODE_SINGLE || MODE == MODE_MMP3 || k >= sp.khf) {
+                                    float e;
+                                    if (pk) e = energy_phase(X, exp_factor_tab(k, sp, etab),
+                                                             k >= sp.khf ? cmul(rot, hrot) : rot, Kc);
+                                    else e = Kc * (X.x * X.x + X.y * X.y);
+                                    if (MODE == MODE_SINGLE) sink.put(k, e);
+                                    else acc[ai] += e;
+                                } else {
+                                    acc[ai] += X.x * X.x + X.y * X.y;
+                                    acc[nwin * nb + ai] += X.x * X.x - X.y * X.y;
+                                    acc[2 * nwin * nb + ai] += 2.0f * X.x * X.y;
+                                }
+                            }
+                            if (phase) rot = cmul(rot, step);
+                        }
+                    }
+                    if (g == 0 && q0 == 0 && Nh < sp.fcount) {
+                        // Nyquist bin k = Nh (a high-frequency bin): X = Re Z[0] - Im Z[0]
+                        const float2 Z0 = buf[pad16(o0)];
+                        const float2 X = make_float2(Z0.x - Z0.y, 0.0f);
+                        const bool pk = Nh < sp.klo || Nh > sp.khi;
+                        const float e = pk ? energy_phase(X, exp_factor_tab(Nh, sp, etab),
+                                                          cmul(centre_rot((unsigned)Nh, m.z, cf, nfu, tw), hrot), Kc)
+                                           : Kc * X.x * X.x;
+                        if (MODE == MODE_SINGLE) sink.put(Nh, e);
+                        else acc[w * nb + L] += e;
+                    }
+                    if (MODE != MODE_SINGLE && last) {
+                        // energies of the accumulated channels
+                        const int nq = (g == 0 && q0 == 0) ? CH + 1 : CH;
+    #pragma unroll 1
+                        for (int h = 0; h < nf; ++h) {
+                            const int rho = h ? rho1 : rho0;
+                            float2 rot = make_float2(1.f, 0.f);
+                            if (phase && MODE == MODE_MMP1) rot = centre_rot((unsigned)(M * q0 + rho), m.z, cf, nfu, tw);
+    #pragma unroll 1
+                            for (int qq = 0; qq < nq; ++qq) {
+                                const bool nyq = qq == CH;
+                                const int q = nyq ? L : q0 + qq;
+                                const int k = nyq ? Nh : M * q + rho;
+                                if (k < sp.fcount && !(nyq && h == 1)) {
+                                    const int ai = w * nb + q + h * L;
+                                    float e;
+                                    if (MODE == MODE_MMP3 || k >= sp.khf) {
+                                        e = acc[ai];
+                                    } else {
+                                        const bool pk = k < sp.klo;
+                                        e = energy_mmp1(acc[ai], make_float2(acc[nwin * nb + ai], acc[2 * nwin * nb + ai]),
+                                                        pk, pk ? exp_factor_tab(k, sp, etab) : 0.0f, rot, sp.K1);
+                                    }
+                                    sink.put(k, e);
+                                }
+                                if (phase && MODE == MODE_MMP1 && !nyq) rot = cmul(rot, step);
+                            }
+                        }
+                    }
+                }
+                if (!COLLECT && (MODE == MODE_SINGLE || last)) {
+                    // max over the lanes of this window (TPW consecutive, aligned lanes);
+                    // non-negative floats order as their bit patterns
+                    unsigned best = __float_as_uint(sink.best);
+                    if (TPW >= 32) {
+                        best = __reduce_max_sync(0xffffffffu, best);
+                        if ((tid & 31) == 0 && valid) atomicMax(s_key + w, best);
+                    } else {
+    #pragma unroll
+                        for (int off = TPW / 2; off; off >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, off));
+                        if ((tid & (TPW - 1)) == 0 && valid) s_key[w] = best;
+                    }
+                }
+            }
+        } else {
+            // (3a) every bin whose energy has no phase term.  A task is q0 .. q0 +
+            // CH - 1 of one window; the tasks holding phase-dependent bins (k < klo
+            // or k > khi) are the first tlo and those from thi on, the same in every
+            // window, and only their phase-dependent bins are left to (3b).
+            for (int base = 0; base < ntasks; base += T) {
+                const int task = base + tid;
+                const bool valid = task < ntasks;
+                const int w = valid ? task / TPW : 0;
+                const int tau = task - w * TPW;
+                const int q0 = tau * CH;
+                BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
+                if (valid) {
+                    const bool phase = tau < tlo || tau >= thi;
+                    const int o0 = (w * nf) << LOGL;
+                    const int o1 = o0 + L;
+#pragma unroll 1
+                    for (int h = 0; h < nf; ++h) {
+                        const int rho = h ? rho1 : rho0;
+                        const float2 wr = h ? wr1 : wr0;
+                        const int oa = h ? o1 : o0;                // A = Y_h[q]
+                        const int ob = pair ? (h ? o0 : o1) : o0;  // B = partner FFT
+                        const int pa = pad16(oa + q0);
+                        // partner L - 1 - q for g >= 1: a descending run inside one
+                        // 16-block, since (L - 1 - q0) mod 16 is 15 or 7
+                        const int pb = pad16(ob + L - 1 - q0);
+                        // W_2L^q: the table entry at q0, then one rotation by W_2L per bin
+                        float2 t = __ldg(tw + (q0 << (12 - LOGL)));
+#pragma unroll 2
+                        for (int qq = 0; qq < CH; ++qq) {
+                            const int q = q0 + qq;
+                            const int k = M * q + rho;
+                            const float2 A = buf[pa + qq];
+                            const float2 Bq = (g == 0) ? buf[pad16(ob + ((L - q) & (L - 1)))] : buf[pb - qq];
+                            const float2 wk = (g == 0) ? t : cmul(wr, t);
+                            t = cmul(t, make_float2(kW2L[LOGL].x, kW2L[LOGL].y));
+                            const float ex = 0.5f * (A.x + Bq.x), ey = 0.5f * (A.y - Bq.y);
+                            const float dx = 0.5f * (A.x - Bq.x), dy = 0.5f * (A.y + Bq.y);
+                            const float2 X = make_float2(ex + wk.x * dy + wk.y * dx, ey + wk.y * dy - wk.x * dx);
+                            if (k < sp.fcount && !(phase && (k < sp.klo || k > sp.khi))) {
+                                const float e = Kc * (X.x * X.x + X.y * X.y);
+                                if (MODE == MODE_SINGLE) sink.put(k, e);
+                                else acc[w * nb + q + h * L] += e;
+                            }
+                        }
+                    }
+                }
+                if (!COLLECT && MODE == MODE_SINGLE) sink_reduce<TPW>(sink.best, s_key, w, valid, tid);
+            }
+            // (3b) the phase-dependent bins (and the Nyquist bin), task by task as in
+            // (3a) but spread over all threads: nph such tasks per window
+            for (int i = tid; i < nwin * nph; i += T) {
+                const int w = i / nph;
+                const int jx = i - w * nph;
+                const int q0 = (jx < tlo ? jx : thi + (jx - tlo)) * CH;
+                BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
                 const int4 m = s_win[w];
                 const float cf = __int_as_float(m.w);
-                const int kmin = M * q0 + (pair ? min(rho0, rho1) : (g == 1 ? rho0 : 0));
-                const int kmax = (g == 0 && q0 == 0) ? Nh
-                                                     : M * (q0 + CH - 1) + (pair ? max(rho0, rho1) : (g == 1 ? rho0 : 0));
-                const bool phase = kmin < sp.klo || kmax > sp.khi;
-                float2 hrot = make_float2(1.f, 0.f), step = make_float2(1.f, 0.f);
-                if (phase) {
-                    float s, cc;
-                    sincospif(-2.0f * s_hf[w], &s, &cc);  // e^{-2 pi i fs t0} for high bins
-                    hrot = make_float2(cc, s);
-                    step = centre_rot((unsigned)M, m.z, cf, nfu, tw);  // psi increment from q to q + 1
-                }
+                float s, cc;
+                sincospif(-2.0f * s_hf[w], &s, &cc);  // e^{-2 pi i fs t0} for high bins
+                const float2 hrot = make_float2(cc, s);
+                const float2 step = centre_rot((unsigned)M, m.z, cf, nfu, tw);  // psi increment from q to q + 1
                 const int o0 = (w * nf) << LOGL;
                 const int o1 = o0 + L;
 #pragma unroll 1
                 for (int h = 0; h < nf; ++h) {
                     const int rho = h ? rho1 : rho0;
                     const float2 wr = h ? wr1 : wr0;
-                    const int oa = h ? o1 : o0;                // A = Y_h[q]
-                    const int ob = pair ? (h ? o0 : o1) : o0;  // B = partner FFT
-                    float2 rot = make_float2(1.f, 0.f);
-                    if (phase) rot = centre_rot((unsigned)(M * q0 + rho), m.z, cf, nfu, tw);
+                    const int oa = h ? o1 : o0;
+                    const int ob = pair ? (h ? o0 : o1) : o0;
+                    float2 rot = centre_rot((unsigned)(M * q0 + rho), m.z, cf, nfu, tw);
                     const int pa = pad16(oa + q0);
+                    const int pb = pad16(ob + L - 1 - q0);
+                    float2 t = __ldg(tw + (q0 << (12 - LOGL)));
 #pragma unroll 2
                     for (int qq = 0; qq < CH; ++qq) {
                         const int q = q0 + qq;
                         const int k = M * q + rho;
                         const float2 A = buf[pa + qq];
-                        const int qb = (g == 0) ? ((L - q) & (L - 1)) : (L - 1 - q);
-                        const float2 Bq = buf[pad16(ob + qb)];
-                        const float2 t = __ldg(tw + (q << (12 - LOGL)));
+                        const float2 Bq = (g == 0) ? buf[pad16(ob + ((L - q) & (L - 1)))] : buf[pb - qq];
                         const float2 wk = (g == 0) ? t : cmul(wr, t);
-                        const float ex = 0.5f * (A.x + Bq.x), ey = 0.5f * (A.y - Bq.y);
-                        const float dx = 0.5f * (A.x - Bq.x), dy = 0.5f * (A.y + Bq.y);
-                        const float2 X = make_float2(ex + wk.x * dy + wk.y * dx, ey + wk.y * dy - wk.x * dx);
-                        if (k < sp.fcount) {
-                            const bool pk = phase && (k < sp.klo || k > sp.khi);
-                            const int ai = w * nb + q + h * L;
-                            if (MODE == MODE_SINGLE || MODE == MODE_MMP3 || k >= sp.khf) {
-                                float e;
-                                if (pk) e = energy_phase(X, exp_factor_tab(k, sp, etab),
-                                                         k >= sp.khf ? cmul(rot, hrot) : rot, Kc);
-                                else e = Kc * (X.x * X.x + X.y * X.y);
-                                if (MODE == MODE_SINGLE) sink.put(k, e);
-                                else acc[ai] += e;
-                            } else {
-                                acc[ai] += X.x * X.x + X.y * X.y;
-                                acc[nwin * nb + ai] += X.x * X.x - X.y * X.y;
-                                acc[2 * nwin * nb + ai] += 2.0f * X.x * X.y;
-                            }
+                        t = cmul(t, make_float2(kW2L[LOGL].x, kW2L[LOGL].y));
+                        if (k < sp.fcount && (k < sp.klo || k > sp.khi)) {
+                            const float ex = 0.5f * (A.x + Bq.x), ey = 0.5f * (A.y - Bq.y);
+                            const float dx = 0.5f * (A.x - Bq.x), dy = 0.5f * (A.y + Bq.y);
+                            const float2 X = make_float2(ex + wk.x * dy + wk.y * dx, ey + wk.y * dy - wk.x * dx);
+                            const float e = energy_phase(X, exp_factor_tab(k, sp, etab), k >= sp.khf ? cmul(rot, hrot) : rot, Kc);
+                            if (MODE == MODE_SINGLE) sink.put(k, e);
+                            else acc[w * nb + q + h * L] += e;
                         }
-                        if (phase) rot = cmul(rot, step);
+                        rot = cmul(rot, step);
                     }
                 }
                 if (g == 0 && q0 == 0 && Nh < sp.fcount) {
@@ -310,47 +532,32 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     if (MODE == MODE_SINGLE) sink.put(Nh, e);
                     else acc[w * nb + L] += e;
                 }
-                if (MODE != MODE_SINGLE && last) {
-                    // energies of the accumulated channels
-                    const int nq = (g == 0 && q0 == 0) ? CH + 1 : CH;
+                if (!COLLECT && MODE == MODE_SINGLE) atomicMax(s_key + w, __float_as_uint(sink.best));
+            }
+            if (MODE == MODE_MMP3 && last) {
+                // energies of the accumulated channels
+                __syncthreads();
+                for (int base = 0; base < ntasks; base += T) {
+                    const int task = base + tid;
+                    const bool valid = task < ntasks;
+                    const int w = valid ? task / TPW : 0;
+                    const int q0 = (task - w * TPW) * CH;
+                    BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
+                    if (valid) {
+                        const int nq = (g == 0 && q0 == 0) ? CH + 1 : CH;
 #pragma unroll 1
-                    for (int h = 0; h < nf; ++h) {
-                        const int rho = h ? rho1 : rho0;
-                        float2 rot = make_float2(1.f, 0.f);
-                        if (phase && MODE == MODE_MMP1) rot = centre_rot((unsigned)(M * q0 + rho), m.z, cf, nfu, tw);
+                        for (int h = 0; h < nf; ++h) {
+                            const int rho = h ? rho1 : rho0;
 #pragma unroll 1
-                        for (int qq = 0; qq < nq; ++qq) {
-                            const bool nyq = qq == CH;
-                            const int q = nyq ? L : q0 + qq;
-                            const int k = nyq ? Nh : M * q + rho;
-                            if (k < sp.fcount && !(nyq && h == 1)) {
-                                const int ai = w * nb + q + h * L;
-                                float e;
-                                if (MODE == MODE_MMP3 || k >= sp.khf) {
-                                    e = acc[ai];
-                                } else {
-                                    const bool pk = k < sp.klo;
-                                    e = energy_mmp1(acc[ai], make_float2(acc[nwin * nb + ai], acc[2 * nwin * nb + ai]),
-                                                    pk, pk ? exp_factor_tab(k, sp, etab) : 0.0f, rot, sp.K1);
-                                }
-                                sink.put(k, e);
+                            for (int qq = 0; qq < nq; ++qq) {
+                                const bool nyq = qq == CH;
+                                const int q = nyq ? L : q0 + qq;
+                                const int k = nyq ? Nh : M * q + rho;
+                                if (k < sp.fcount && !(nyq && h == 1)) sink.put(k, acc[w * nb + q + h * L]);
                             }
-                            if (phase && MODE == MODE_MMP1 && !nyq) rot = cmul(rot, step);
                         }
                     }
-                }
-            }
-            if (!COLLECT && (MODE == MODE_SINGLE || last)) {
-                // max over the lanes of this window (TPW consecutive, aligned lanes);
-                // non-negative floats order as their bit patterns
-                unsigned best = __float_as_uint(sink.best);
-                if (TPW >= 32) {
-                    best = __reduce_max_sync(0xffffffffu, best);
-                    if ((tid & 31) == 0 && valid) atomicMax(s_key + w, best);
-                } else {
-#pragma unroll
-                    for (int off = TPW / 2; off; off >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, off));
-                    if ((tid & (TPW - 1)) == 0 && valid) s_key[w] = best;
+                    if (!COLLECT) sink_reduce<TPW>(sink.best, s_key, w, valid, tid);
                 }
             }
         }
