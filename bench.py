@@ -212,13 +212,24 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def profiled_traffic():
-    """dram bytes per refresh launch from the committed ncu summary, if any."""
+def profiled_traffic(w):
+    """DRAM bytes of one refresh fork of the headline workload, from the
+    committed ncu summary (cold-cache capture of one epoch, scaled by the
+    epochs); None for other workloads."""
+    import re
+
+    if w.name != "mmp2-19x8x5120@256" or len(w.epochs) != 8:
+        return None
     try:
-        with open(os.path.join(ROOT, "profiles", "refresh_traffic.json")) as f:
-            return json.load(f)
+        with open(os.path.join(ROOT, "profiles", "refresh_traffic_mmp2_1epoch.md")) as f:
+            text = f.read()
     except OSError:
         return None
+    one = re.search(r"dram_bytes_per_fork_one_epoch: (\d+)", text)
+    scale = re.search(r"dram_bytes_per_fork_scale_to_bench: (\d+)", text)
+    if not one or not scale:
+        return None
+    return float(one.group(1)) * float(scale.group(1))
 
 
 def ours(args):
@@ -326,11 +337,13 @@ def ours(args):
         flops_per_launch = st.fft_flops / max(1, st.refresh_launches)
         peaks, peak_kind = measured_peaks()
         achieved_gbs = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
-        tr = profiled_traffic()
+        tr = profiled_traffic(w)
         roofline = {"kernel": "k_refresh (windowed FFT + energy + slot max)", "bound": "hbm",
                     "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                     "frac": achieved_gbs / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs",
-                    "traffic": tr.get("dram_bytes_per_launch") if tr else None,
+                    "traffic": tr, "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum, cold "
+                                                      "cache, one epoch scaled to 8 (profiles/"
+                                                      "refresh_traffic_mmp2_1epoch.md)") if tr else None,
                     "launch_ms": per_launch_ms, "launches": st.refresh_launches,
                     "algorithmic_bytes_per_launch": bytes_per_launch}
         fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12

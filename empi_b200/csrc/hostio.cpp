@@ -1,7 +1,7 @@
 // Host surface kept from empi: the key/value config file, the float32 signal
 // reader, the SVAROG (MPv5) book writer and the CLI driver with its stdout
-// progress protocol.  Decomposition itself is one batched device run over all
-// epochs read from the file.
+// progress protocol.  Epochs stream through the device in batches, the next
+// batch read from the file while the current one decomposes.
 #include <algorithm>
 #include <cctype>
 #include <climits>
@@ -17,12 +17,15 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/empi_b200.h"
 #include "engine.hpp"
 
 namespace {
+
+constexpr int kStreamEpochs = 64;  // epochs per device batch unless the config says otherwise
 
 struct Error : std::runtime_error {
     empi_status status;
@@ -303,71 +306,121 @@ void run_config(const char* configPath, const empi_engine_opts* opts) {
     const std::string bookPath = conf.at("nameOfOutputDirectory") + "/" + prefix + "_" + typeOfMP + ".b";
     write_file(bookPath, {}, false);  // BookWriter opens (truncates) the file up front
 
-    // read every epoch first; a read error ends the job after the epochs
-    // before it are decomposed and written, as in the reference's loop
-    std::vector<std::vector<float>> epochs;
+    // Epochs stream through the GPU in batches of gpuEpochsPerBatch (an
+    // optional key the reference ignores; default kStreamEpochs): while one
+    // batch decomposes on a worker thread, the next is read from the file, and
+    // each batch's protocol lines and book blocks are written as soon as it
+    // ends.  A read error ends the job after the epochs before it are
+    // decomposed and written, as in the reference's epoch loop.
+    int perBatch = conf.has("gpuEpochsPerBatch") ? atoi(conf.at("gpuEpochsPerBatch").c_str()) : kStreamEpochs;
+    if (perBatch <= 0) throw Error(EMPI_ERR_CONFIG, "invalidGpuEpochsPerBatch");
+    struct Chunk {
+        std::vector<std::vector<float>> epochs;
+        std::unique_ptr<Error> pending;  // read error after these epochs
+    };
     int N = 0;
-    std::unique_ptr<Error> pending;
-    try {
-        for (;;) {
-            int count = 0;
-            std::vector<float> e = reader->read(count);
-            if (!count) break;
-            if (epochs.empty()) N = count;
-            if (count != N) throw Error(EMPI_ERR_IO, "fileIsTruncated");
-            epochs.push_back(std::move(e));
+    auto readChunk = [&](Chunk& ch) {
+        ch.epochs.clear();
+        ch.pending.reset();
+        try {
+            while ((int)ch.epochs.size() < perBatch) {
+                int count = 0;
+                std::vector<float> e = reader->read(count);
+                if (!count) break;
+                if (N == 0) N = count;
+                if (count != N) throw Error(EMPI_ERR_IO, "fileIsTruncated");
+                ch.epochs.push_back(std::move(e));
+            }
+        } catch (const Error& e) {
+            ch.pending.reset(new Error(e));
         }
-    } catch (const Error& e) {
-        pending.reset(new Error(e));
-    }
+    };
 
-    std::vector<uint8_t> book;
-    if (!epochs.empty()) {
-        empi_engine* eng = nullptr;
-        check(empi_engine_create(opts, &eng));
-        std::unique_ptr<empi_engine, void (*)(empi_engine*)> eg(eng, empi_engine_destroy);
+    Chunk cur, next;
+    readChunk(cur);
+    empi_engine* eng = nullptr;
+    std::unique_ptr<empi_engine, void (*)(empi_engine*)> eg(nullptr, empi_engine_destroy);
+    std::unique_ptr<empi_batch, void (*)(empi_batch*)> bg(nullptr, empi_batch_destroy);
+    int batchEpochs = 0;
+    uint64_t atomCount = 0;
+    const int cap = settings.iteration_max;
+    const bool smp = variant == EMPI_SMP;
+    const int loops = smp ? C : 1;
+    std::vector<float> chanMajor;
+    int epochNumber = 0;
+    while (!cur.epochs.empty()) {
+        if (!eng) {
+            check(empi_engine_create(opts, &eng));
+            eg.reset(eng);
+            check(empi_dictionary_size(&dict, reader->freqSampling, N, &atomCount, nullptr));
+            chanMajor.resize((size_t)C * N);
+        }
+        const int count = (int)cur.epochs.size();
         std::vector<empi_epoch> eps;
-        for (auto& e : epochs) eps.push_back(empi_epoch{reader->freqSampling, C, N, e.data()});
-        empi_batch* batch = nullptr;
-        check(empi_batch_create(eng, variant, &dict, &settings, eps.data(), (int)eps.size(), &batch));
-        std::unique_ptr<empi_batch, void (*)(empi_batch*)> bg(batch, empi_batch_destroy);
-        check(empi_batch_load(batch, eps.data()));
-        check(empi_batch_run(batch));
-        uint64_t atomCount = 0;
-        check(empi_dictionary_size(&dict, reader->freqSampling, N, &atomCount, nullptr));
-        const int cap = settings.iteration_max;
-        const bool smp = variant == EMPI_SMP;
-        const int loops = smp ? C : 1;
-        std::vector<double> atoms((size_t)C * cap * 6), energies((size_t)loops * cap), totals(loops);
-        std::vector<int> counts(C);
-        std::vector<float> chanMajor((size_t)C * N);
-        for (size_t e = 0; e < epochs.size(); ++e) {
-            check(empi_batch_atoms(batch, (int)e, cap, atoms.data(), counts.data(), energies.data(), nullptr));
-            check(empi_batch_total_energy(batch, (int)e, totals.data()));
+        for (auto& e : cur.epochs) eps.push_back(empi_epoch{reader->freqSampling, C, N, e.data()});
+        // results of this batch, filled by the worker
+        std::vector<double> atoms((size_t)count * C * cap * 6), energies((size_t)count * loops * cap),
+            totals((size_t)count * loops);
+        std::vector<int> counts((size_t)count * C);
+        std::exception_ptr failure;
+        std::thread worker([&] {
+            try {
+                if (!bg || batchEpochs != count) {
+                    empi_batch* batch = nullptr;
+                    bg.reset();
+                    check(empi_batch_create(eng, variant, &dict, &settings, eps.data(), count, &batch));
+                    bg.reset(batch);
+                    batchEpochs = count;
+                }
+                check(empi_batch_load(bg.get(), eps.data()));
+                check(empi_batch_run(bg.get()));
+                for (int e = 0; e < count; ++e) {
+                    check(empi_batch_atoms(bg.get(), e, cap, atoms.data() + (size_t)e * C * cap * 6,
+                                           counts.data() + (size_t)e * C, energies.data() + (size_t)e * loops * cap,
+                                           nullptr));
+                    check(empi_batch_total_energy(bg.get(), e, totals.data() + (size_t)e * loops));
+                }
+            } catch (...) {
+                failure = std::current_exception();
+            }
+        });
+        if (!cur.pending) readChunk(next);  // overlaps the device run
+        worker.join();
+        if (failure) std::rethrow_exception(failure);
+
+        std::vector<uint8_t> book;
+        for (int e = 0; e < count; ++e) {
+            ++epochNumber;
+            const double* at = atoms.data() + (size_t)e * C * cap * 6;
+            const int* cn = counts.data() + (size_t)e * C;
+            const double* en = energies.data() + (size_t)e * loops * cap;
+            const double* tot = totals.data() + (size_t)e * loops;
             // src/empi.cpp:159 and src/classes.cpp:41-48
-            std::cout << "START" << '\t' << (e + 1) << '\t' << C << '\t' << settings.iteration_max << '\t'
+            std::cout << "START" << '\t' << epochNumber << '\t' << C << '\t' << settings.iteration_max << '\t'
                       << 100 * (1 - settings.residual_energy) << std::endl;
             for (int l = 0; l < loops; ++l) {
                 if (smp) std::cout << "CHANNEL\t" << l << std::endl;
-                const int n = counts[smp ? l : 0];
-                double residue = totals[l];
+                const int n = cn[smp ? l : 0];
+                double residue = tot[l];
                 for (int it = 1; it <= n; ++it) {
-                    double energyProgress = 100.0 * (1.0 - residue / totals[l]);
-                    double totalProgress =
-                        std::max(100.0 * (it - 1) / settings.iteration_max, energyProgress);
+                    double energyProgress = 100.0 * (1.0 - residue / tot[l]);
+                    double totalProgress = std::max(100.0 * (it - 1) / settings.iteration_max, energyProgress);
                     std::cout << "ATOM\t" << (it - 1) << '\t' << atomCount << '\t' << energyProgress << '\t'
                               << totalProgress << std::endl;
-                    residue = energies[(size_t)l * cap + it - 1];
+                    residue = en[(size_t)l * cap + it - 1];
                 }
             }
             for (int c = 0; c < C; ++c)
-                for (int i = 0; i < N; ++i) chanMajor[(size_t)c * N + i] = epochs[e][(size_t)i * C + c];
-            if (e == 0) book_header(book, C, reader->freqSampling);
-            book_epoch(book, (int)e + 1, C, N, chanMajor.data(), cap, atoms.data(), counts.data());
+                for (int i = 0; i < N; ++i) chanMajor[(size_t)c * N + i] = cur.epochs[e][(size_t)i * C + c];
+            if (epochNumber == 1) book_header(book, C, reader->freqSampling);
+            book_epoch(book, epochNumber, C, N, chanMajor.data(), cap, at, cn);
         }
+        write_file(bookPath, book, true);
+        if (cur.pending) throw *cur.pending;
+        std::swap(cur, next);
+        next.epochs.clear();
     }
-    write_file(bookPath, book, false);
-    if (pending) throw *pending;
+    if (cur.pending) throw *cur.pending;
     puts(" END");
 }
 

@@ -217,3 +217,37 @@ def test_cli_book_matches_reference(tmp_path):
     assert len(ga) == len(ra) == 50
     for g, r in zip(ga, ra):
         assert all(abs(a - b) <= 2e-5 * max(1.0, abs(b)) for a, b in zip(g[:5], r[:5]))
+
+
+@pytest.mark.parametrize("variant", ["MMP2", "SMP"])
+def test_cli_streams_epochs_in_batches(tmp_path, variant):
+    """Epochs stream through the device in batches (gpuEpochsPerBatch): the
+    protocol lines and the book are the same bytes whatever the batch size,
+    and a truncated last epoch still ends the job with fileIsTruncated after
+    the complete epochs are written (src/empi.cpp:148-164, src/io.cpp:48-55)."""
+    from empi_b200 import synth
+
+    w = synth.workload(1, epochs=5, channels=3, samples=700, seed=11)
+    data = np.concatenate([e.reshape(-1) for e in w.epochs]).astype(np.float32)
+    cli = os.path.join(os.path.dirname(empi_b200.LIB_PATH), "empi-gpu")
+    outs = {}
+    for per, trunc in ((1, False), (2, False), (64, False), (2, True)):
+        d = tmp_path / f"b{per}{'t' if trunc else ''}"
+        d.mkdir()
+        (data[:-5] if trunc else data).tofile(d / "sig.bin")
+        (d / "run.cfg").write_text(
+            f"energyError 0.01\nmaximalNumberOfIterations 12\nenergyPercent 99.0\nMP {variant}\n"
+            f"nameOfDataFile sig.bin\nnameOfOutputDirectory .\nsamplingFrequency {w.fs}\n"
+            f"numberOfChannels 3\nselectedChannels 1-3\nnumberOfSamplesInEpoch 700\n"
+            f"gpuEpochsPerBatch {per}\n")
+        p = subprocess.run([cli, "run.cfg"], cwd=d, capture_output=True, text=True, timeout=300)
+        outs[(per, trunc)] = (p.returncode, p.stdout, (d / f"sig_{variant.lower()[:3]}.b").read_bytes())
+    rc, out, book = outs[(64, False)]
+    assert rc == 0 and out.count("START") == 5 and out.rstrip().endswith("END")
+    for per in (1, 2):
+        assert outs[(per, False)] == (rc, out, book)
+    rc_t, out_t, book_t = outs[(2, True)]
+    assert rc_t != 0 and "ERROR\tfileIsTruncated" in out_t
+    assert out_t.count("START") == 4
+    # the four complete epochs are written as in the full run
+    assert book.startswith(book_t) and len(book_t) < len(book)
