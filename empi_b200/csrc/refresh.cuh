@@ -19,6 +19,7 @@ constexpr int kVPT = kUnitPoints / kUnitThreads;
 constexpr int kBufFloat2 = kUnitPoints + kUnitPoints / 16 + 16;
 constexpr int kAccBins = kUnitPoints + kMaxWindowsPerUnit;
 constexpr int kBinsPerTask = 8;  // consecutive q per thread in the spectrum stage
+constexpr int kEtabSmem = 512;   // expFactor entries of one scale staged in shared memory
 
 // W_2L = exp(-i pi / L) for L = 2^0 .. 2^13 (cos and -sin of pi / L, rounded to
 // float): the step of the spectrum stage's twiddle W_2L^q from bin q to q + 1.
@@ -46,9 +47,10 @@ constexpr Rot kW2L[14] = {
 struct RefreshSmem {
     static constexpr size_t buf = 0;
     static constexpr size_t win = buf + sizeof(float2) * kBufFloat2;          // int4 (iL, W, ci, cf bits)
-    static constexpr size_t hf = win + sizeof(int4) * kMaxWindowsPerUnit;     // float
-    static constexpr size_t key = hf + sizeof(float) * kMaxWindowsPerUnit;    // u32 energy bits
-    static constexpr size_t acc = key + sizeof(unsigned) * kMaxWindowsPerUnit;
+    static constexpr size_t rot = win + sizeof(int4) * kMaxWindowsPerUnit;    // float4 (hrot, step)
+    static constexpr size_t key = rot + sizeof(float4) * kMaxWindowsPerUnit;  // u32 energy bits
+    static constexpr size_t etab = key + sizeof(unsigned) * kMaxWindowsPerUnit;  // float, kEtabSmem
+    static constexpr size_t acc = etab + sizeof(float) * kEtabSmem;
 };
 
 template <int MODE>
@@ -68,11 +70,6 @@ __device__ __forceinline__ float2 centre_rot(unsigned kk, int ci, float cf, unsi
     float s, c;
     sincospif(2.0f * (2.0f * (float)kk * cf / (float)nf), &s, &c);
     return cmul(a, make_float2(c, s));
-}
-
-// expFactor of a phase-dependent bin (k < klo or k > khi), src/gabor.cpp:51
-__device__ __forceinline__ float exp_factor_tab(int k, const ScalePlan& sp, const float* __restrict__ etab) {
-    return __ldg(etab + sp.eoff + (k < sp.klo ? k : sp.klo + (k - sp.khi - 1)));
 }
 
 // fs |v|^2 normReal^2 of one channel (GaborComputer::compute,
@@ -160,7 +157,8 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
     constexpr int TPW = L / CH;                                // tasks per window
     float2* buf = reinterpret_cast<float2*>(smem + RefreshSmem::buf);
     int4* s_win = reinterpret_cast<int4*>(smem + RefreshSmem::win);
-    float* s_hf = reinterpret_cast<float*>(smem + RefreshSmem::hf);
+    float4* s_rot = reinterpret_cast<float4*>(smem + RefreshSmem::rot);
+    float* s_etab = reinterpret_cast<float*>(smem + RefreshSmem::etab);
     unsigned* s_key = reinterpret_cast<unsigned*>(smem + RefreshSmem::key);
     float* acc = reinterpret_cast<float*>(smem + RefreshSmem::acc);
 
@@ -177,17 +175,31 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
     const int rho0 = r, rho1 = M - r;                       // residues of the group's FFTs
     const int tid = threadIdx.x, T = blockDim.x;
     const float2* __restrict__ tw = b.tw;
-    const float* __restrict__ etab = b.etab;
     const float aG2 = sp.aG2, Kc = sp.Kc;
 
+    // Per window: geometry, and for the phase-dependent bins e^{-2 pi i fs t0}
+    // (high bins) and the step of psi from q to q + 1; the scale's expFactor
+    // table when it fits.  Read by the spectrum stage instead of global loads
+    // and transcendentals inside its tasks.
+    const int ecount = sp.klo + (sp.fcount - 1 - sp.khi);
+    const bool etab_smem = ecount <= kEtabSmem;
     {
         const long long w0 = sp.win_base + t_start;
         for (int w = tid; w < nwin; w += T) {
-            s_win[w] = __ldg(b.wtab + w0 + w);
-            s_hf[w] = __ldg(b.whf + w0 + w);
+            const int4 m = __ldg(b.wtab + w0 + w);
+            s_win[w] = m;
+            float sh, ch;
+            sincospif(-2.0f * __ldg(b.whf + w0 + w), &sh, &ch);
+            const float2 st = centre_rot((unsigned)sp.M, m.z, __int_as_float(m.w), (unsigned)sp.nfft, b.tw);
+            s_rot[w] = make_float4(ch, sh, st.x, st.y);
             s_key[w] = 0u;
         }
+        if (etab_smem)
+            for (int i = tid; i < ecount; i += T) s_etab[i] = __ldg(b.etab + sp.eoff + i);
     }
+    const float* __restrict__ etv = etab_smem ? s_etab : b.etab + sp.eoff;
+    // expFactor of a phase-dependent bin (k < klo or k > khi), src/gabor.cpp:51
+    auto efac = [&](int k) { return etv[k < sp.klo ? k : sp.klo + (k - sp.khi - 1)]; };
     float2 wr0 = make_float2(1.f, 0.f), wr1 = make_float2(1.f, 0.f);  // W_Nfft^rho
     if (g >= 1) {
         float s0, c0;
@@ -322,10 +334,9 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     const bool phase = kmin < sp.klo || kmax > sp.khi;
                     float2 hrot = make_float2(1.f, 0.f), step = make_float2(1.f, 0.f);
                     if (phase) {
-                        float s, cc;
-                        sincospif(-2.0f * s_hf[w], &s, &cc);  // e^{-2 pi i fs t0} for high bins
-                        hrot = make_float2(cc, s);
-                        step = centre_rot((unsigned)M, m.z, cf, nfu, tw);  // psi increment from q to q + 1
+                        const float4 hr = s_rot[w];
+                        hrot = make_float2(hr.x, hr.y);  // e^{-2 pi i fs t0} for high bins
+                        step = make_float2(hr.z, hr.w);  // psi increment from q to q + 1
                     }
                     const int o0 = (w * nf) << LOGL;
                     const int o1 = o0 + L;
@@ -359,7 +370,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                                 const int ai = w * nb + q + h * L;
                                 if (MODE == MODE_SINGLE || MODE == MODE_MMP3 || k >= sp.khf) {
                                     float e;
-                                    if (pk) e = energy_phase(X, exp_factor_tab(k, sp, etab),
+                                    if (pk) e = energy_phase(X, efac(k),
                                                              k >= sp.khf ? cmul(rot, hrot) : rot, Kc);
                                     else e = Kc * (X.x * X.x + X.y * X.y);
                                     if (MODE == MODE_SINGLE) sink.put(k, e);
@@ -378,7 +389,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                         const float2 Z0 = buf[pad16(o0)];
                         const float2 X = make_float2(Z0.x - Z0.y, 0.0f);
                         const bool pk = Nh < sp.klo || Nh > sp.khi;
-                        const float e = pk ? energy_phase(X, exp_factor_tab(Nh, sp, etab),
+                        const float e = pk ? energy_phase(X, efac(Nh),
                                                           cmul(centre_rot((unsigned)Nh, m.z, cf, nfu, tw), hrot), Kc)
                                            : Kc * X.x * X.x;
                         if (MODE == MODE_SINGLE) sink.put(Nh, e);
@@ -405,7 +416,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                                     } else {
                                         const bool pk = k < sp.klo;
                                         e = energy_mmp1(acc[ai], make_float2(acc[nwin * nb + ai], acc[2 * nwin * nb + ai]),
-                                                        pk, pk ? exp_factor_tab(k, sp, etab) : 0.0f, rot, sp.K1);
+                                                        pk, pk ? efac(k) : 0.0f, rot, sp.K1);
                                     }
                                     sink.put(k, e);
                                 }
@@ -486,10 +497,9 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                 BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
                 const int4 m = s_win[w];
                 const float cf = __int_as_float(m.w);
-                float s, cc;
-                sincospif(-2.0f * s_hf[w], &s, &cc);  // e^{-2 pi i fs t0} for high bins
-                const float2 hrot = make_float2(cc, s);
-                const float2 step = centre_rot((unsigned)M, m.z, cf, nfu, tw);  // psi increment from q to q + 1
+                const float4 hr = s_rot[w];
+                const float2 hrot = make_float2(hr.x, hr.y);  // e^{-2 pi i fs t0} for high bins
+                const float2 step = make_float2(hr.z, hr.w);  // psi increment from q to q + 1
                 const int o0 = (w * nf) << LOGL;
                 const int o1 = o0 + L;
 #pragma unroll 1
@@ -514,7 +524,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                             const float ex = 0.5f * (A.x + Bq.x), ey = 0.5f * (A.y - Bq.y);
                             const float dx = 0.5f * (A.x - Bq.x), dy = 0.5f * (A.y + Bq.y);
                             const float2 X = make_float2(ex + wk.x * dy + wk.y * dx, ey + wk.y * dy - wk.x * dx);
-                            const float e = energy_phase(X, exp_factor_tab(k, sp, etab), k >= sp.khf ? cmul(rot, hrot) : rot, Kc);
+                            const float e = energy_phase(X, efac(k), k >= sp.khf ? cmul(rot, hrot) : rot, Kc);
                             if (MODE == MODE_SINGLE) sink.put(k, e);
                             else acc[w * nb + q + h * L] += e;
                         }
@@ -526,7 +536,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     const float2 Z0 = buf[pad16(o0)];
                     const float2 X = make_float2(Z0.x - Z0.y, 0.0f);
                     const bool pk = Nh < sp.klo || Nh > sp.khi;
-                    const float e = pk ? energy_phase(X, exp_factor_tab(Nh, sp, etab),
+                    const float e = pk ? energy_phase(X, efac(Nh),
                                                       cmul(centre_rot((unsigned)Nh, m.z, cf, nfu, tw), hrot), Kc)
                                        : Kc * X.x * X.x;
                     if (MODE == MODE_SINGLE) sink.put(Nh, e);
