@@ -239,11 +239,39 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
         thi = max(lo, tlo);
     }
     const int nph = tlo + (TPW - thi);
+    // Twiddles of the load, per unit: the twist of residue group g at input
+    // index n is W_Nh^{r n} (a pair's two residues r, M - r use it and its
+    // conjugate) or W_2L^n (g = 1, residue M/2); a pair's second FFT input is
+    // also multiplied by W_L^n.  A thread's points step through n by fixed
+    // strides, so one table lookup per window or job is followed by
+    // rotations.
     for (int c = 0; c < ip.C; ++c) {
         const float* __restrict__ x = b.residual32 + ip.res_off + (long long)c * dp.N;
+        const float2 one = make_float2(1.f, 0.f);
+        auto twist = [&](int n) -> float2 {
+            if (g == 1) return __ldg(tw + ((n & (2 * L - 1)) << (12 - LOGL)));
+            const unsigned rn = ((unsigned)r * (unsigned)n) & (unsigned)(Nh - 1);
+            return twiddle_pow2(rn, (unsigned)Nh, tw);
+        };
+        auto pfac = [&](int n) -> float2 { return __ldg(tw + ((n & (L - 1)) << (13 - LOGL))); };
+        // step from fold m to m + 1 (n + L): W_2L^L = -1, or W_Nh^{r L}
+        const float2 fold = g == 0 ? one : (g == 1 ? make_float2(-1.f, 0.f) : twist(L));
+        constexpr int FIRST = LOGL & 3;  // log2 of the odd first radix; 0: radix-16 passes only
+        constexpr int R0 = 1 << FIRST;
+        constexpr int LQ = LOGL - FIRST;  // log2 of L / R0
+        // fused first pass: a job's points are jq + rr L / R0
+        const float2 jstep = (FIRST != 0 && g >= 1) ? twist(1 << LQ) : one;
+        const float2 jpstep = (FIRST != 0 && pair) ? pfac(1 << LQ) : one;
+        // other sizes: a thread's points are np0 + i T within a window
+        const int np0 = tid & (L - 1);
+        const float2 t0 = (FIRST == 0 && g >= 1) ? twist(np0) : one;
+        const float2 p0 = (FIRST == 0 && pair) ? pfac(np0) : one;
+        const float2 tstep = (FIRST == 0 && g >= 1 && L > kUnitThreads) ? twist(kUnitThreads) : one;
+        const float2 pstep = (FIRST == 0 && pair && L > kUnitThreads) ? pfac(kUnitThreads) : one;
         // (1) load: y_r[n'] = sum_m z[n' + mL] W_Nh^{r (n' + mL)}; for the second
-        // FFT of a pair the sum is conjugate-twisted and multiplied by W_L^{n'}
-        auto load_point = [&](const int4& m, float cf, int np, float2& a1, float2& a2) {
+        // FFT of a pair the sum is conjugate-twisted (and then multiplied by
+        // W_L^{n'} by the caller).  t = the twist at n = np.
+        auto load_point = [&](const int4& m, float cf, int np, float2 t, float2& a1, float2& a2) {
             const float* __restrict__ xs = x + m.x;
             a1 = make_float2(0.f, 0.f);
             a2 = make_float2(0.f, 0.f);
@@ -259,30 +287,34 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                 if (g == 0) {
                     a1 = cadd(a1, z);
                 } else if (g == 1) {
-                    // W_Nh^{(M/2) n} = W_{2L}^{n}
-                    a1 = cadd(a1, cmul(z, __ldg(tw + ((n & (2 * L - 1)) << (12 - LOGL)))));
+                    a1 = cadd(a1, cmul(z, t));
+                    t = make_float2(-t.x, -t.y);
                 } else {
-                    const unsigned rn = ((unsigned)r * (unsigned)n) & (unsigned)(Nh - 1);
-                    const float2 t = twiddle_pow2(rn, (unsigned)Nh, tw);
                     a1 = cadd(a1, cmul(z, t));
                     a2 = cadd(a2, cmulc(z, t));
+                    t = cmul(t, fold);
                 }
             }
-            if (pair) a2 = cmul(a2, __ldg(tw + (np << (13 - LOGL))));
         };
-        constexpr int FIRST = LOGL & 3;  // log2 of the odd first radix; 0: radix-16 passes only
         if constexpr (FIRST != 0) {
             // the first Stockham pass (radix 2^FIRST, no twiddles) fused into the load
-            constexpr int R0 = 1 << FIRST;
-            constexpr int LQ = LOGL - FIRST;  // log2 of L / R0
             for (int job = tid; job < (nwin << LQ); job += T) {
                 const int w = job >> LQ;
                 const int jq = job & ((1 << LQ) - 1);
                 const int4 m = s_win[w];
                 const float cf = __int_as_float(m.w);
+                float2 t = g >= 1 ? twist(jq) : one;
+                float2 pf = pair ? pfac(jq) : one;
                 float2 v1[R0], v2[R0];
 #pragma unroll
-                for (int rr = 0; rr < R0; ++rr) load_point(m, cf, jq + (rr << LQ), v1[rr], v2[rr]);
+                for (int rr = 0; rr < R0; ++rr) {
+                    load_point(m, cf, jq + (rr << LQ), t, v1[rr], v2[rr]);
+                    if (pair) v2[rr] = cmul(v2[rr], pf);
+                    if (rr + 1 < R0) {
+                        t = cmul(t, jstep);
+                        pf = cmul(pf, jpstep);
+                    }
+                }
                 const int o = ((w * nf) << LOGL) + jq * R0;
                 dft<R0>(v1);
 #pragma unroll
@@ -296,15 +328,24 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
             __syncthreads();
             fft_batch_rest<kVPT, kTwN, LOGL>(buf, (nwin * nf) << LOGL, tw);
         } else {
+            float2 t = t0, pf = p0;
             for (int idx = tid; idx < (nwin << LOGL); idx += T) {
                 const int w = idx >> LOGL;
                 const int np = idx & (L - 1);
+                if (np == np0) {  // first point of the thread in a window
+                    t = t0;
+                    pf = p0;
+                }
                 const int4 m = s_win[w];
                 float2 a1, a2;
-                load_point(m, __int_as_float(m.w), np, a1, a2);
+                load_point(m, __int_as_float(m.w), np, t, a1, a2);
                 const int o = (w * nf) << LOGL;
                 buf[pad16(o + np)] = a1;
-                if (pair) buf[pad16(o + L + np)] = a2;
+                if (pair) buf[pad16(o + L + np)] = cmul(a2, pf);
+                if (L > kUnitThreads) {
+                    t = cmul(t, tstep);
+                    pf = cmul(pf, pstep);
+                }
             }
             __syncthreads();
             // (2) FFT of every sub-sequence in the unit
