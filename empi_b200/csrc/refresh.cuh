@@ -328,23 +328,34 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
             __syncthreads();
             fft_batch_rest<kVPT, kTwN, LOGL>(buf, (nwin * nf) << LOGL, tw);
         } else {
-            float2 t = t0, pf = p0;
-            for (int idx = tid; idx < (nwin << LOGL); idx += T) {
-                const int w = idx >> LOGL;
-                const int np = idx & (L - 1);
-                if (np == np0) {  // first point of the thread in a window
-                    t = t0;
-                    pf = p0;
+            if constexpr (L > kUnitThreads) {
+                // a window at a time: its geometry read once, the twist rotated
+                // from point to point (np0 + i T)
+                for (int w = 0; w < nwin; ++w) {
+                    const int4 m = s_win[w];
+                    const float cf = __int_as_float(m.w);
+                    const int o = (w * nf) << LOGL;
+                    float2 t = t0, pf = p0;
+#pragma unroll 2
+                    for (int np = np0; np < L; np += kUnitThreads) {
+                        float2 a1, a2;
+                        load_point(m, cf, np, t, a1, a2);
+                        buf[pad16(o + np)] = a1;
+                        if (pair) buf[pad16(o + L + np)] = cmul(a2, pf);
+                        t = cmul(t, tstep);
+                        pf = cmul(pf, pstep);
+                    }
                 }
-                const int4 m = s_win[w];
-                float2 a1, a2;
-                load_point(m, __int_as_float(m.w), np, t, a1, a2);
-                const int o = (w * nf) << LOGL;
-                buf[pad16(o + np)] = a1;
-                if (pair) buf[pad16(o + L + np)] = cmul(a2, pf);
-                if (L > kUnitThreads) {
-                    t = cmul(t, tstep);
-                    pf = cmul(pf, pstep);
+            } else {
+                for (int idx = tid; idx < (nwin << LOGL); idx += T) {
+                    const int w = idx >> LOGL;
+                    const int np = idx & (L - 1);
+                    const int4 m = s_win[w];
+                    float2 a1, a2;
+                    load_point(m, __int_as_float(m.w), np, t0, a1, a2);
+                    const int o = (w * nf) << LOGL;
+                    buf[pad16(o + np)] = a1;
+                    if (pair) buf[pad16(o + L + np)] = cmul(a2, p0);
                 }
             }
             __syncthreads();
