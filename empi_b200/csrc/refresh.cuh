@@ -370,7 +370,100 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
         // faster; MMP1 folds the phase into its channel sums.  Those keep the
         // single pass.
         constexpr bool kSplit = MODE != MODE_MMP1 && LOGL >= 6 && LOGL <= 11;
-        if constexpr (!kSplit) {
+        if constexpr (!kSplit && LOGL == 12 && MODE == MODE_SINGLE) {
+            // Mirrored pairs: bins k and Nh - k read the same two values
+            // (Z[k], Z[Nh - k]) with A and B exchanged, so one pair of loads
+            // gives both.  A task takes q0 .. q0 + nq - 1 and their mirrors: the
+            // partner residue's L - 1 - q (pairs, g = 1) or L - q (g = 0, where
+            // q = 0 also gives the Nyquist bin and the last task adds q = L/2).
+            constexpr int QH = CH / 2;
+            for (int base = 0; base < ntasks; base += T) {
+                const int task = base + tid;
+                const bool valid = task < ntasks;
+                const int w = valid ? task / TPW : 0;
+                const int tau = task - w * TPW;
+                BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
+                if (valid) {
+                    const int4 m = s_win[w];
+                    const float cf = __int_as_float(m.w);
+                    const int nq = pair ? CH : QH;
+                    const int q0 = tau * nq;
+                    const int kmin = M * q0 + rho0, kmax = M * (q0 + nq - 1) + rho0;
+                    const bool phase = kmin < sp.klo || kmax > sp.khi || Nh - kmax < sp.klo || Nh - kmin > sp.khi;
+                    float2 hrot = make_float2(1.f, 0.f), step = make_float2(1.f, 0.f), ew = make_float2(1.f, 0.f);
+                    float2 rot = make_float2(1.f, 0.f);
+                    if (phase) {
+                        const float4 hr = s_rot[w];
+                        hrot = make_float2(hr.x, hr.y);
+                        step = make_float2(hr.z, hr.w);
+                        float se, ce;
+                        sincospif(2.0f * cf, &se, &ce);  // e^{i 2 pi c}: e^{i psi(Nh - k)} = e^{i 2 pi c} conj(e^{i psi(k)})
+                        ew = make_float2(ce, se);
+                        rot = centre_rot((unsigned)kmin, m.z, cf, nfu, tw);
+                    }
+                    const int o0 = (w * nf) << LOGL;
+                    const int ob = pair ? o0 + L : o0;  // the partner residue's FFT
+                    float2 t = __ldg(tw + (q0 << (12 - LOGL)));  // W_2L^q
+#pragma unroll 2
+                    for (int qq = 0; qq < nq; ++qq) {
+                        const int q = q0 + qq;
+                        const int k = M * q + rho0;
+                        const int km = Nh - k;
+                        const float2 A = buf[pad16(o0 + q)];
+                        const float2 Bq = (g == 0) ? buf[pad16(o0 + ((L - q) & (L - 1)))] : buf[pad16(ob + L - 1 - q)];
+                        const float2 tn = cmul(t, make_float2(kW2L[LOGL].x, kW2L[LOGL].y));  // W_2L^{q+1}
+                        // W_2L^{L-q} = -conj(W_2L^q); W_2L^{L-1-q} = -conj(W_2L^{q+1})
+                        const float2 tm = (g == 0) ? make_float2(-t.x, t.y) : make_float2(-tn.x, tn.y);
+                        const float2 wk = (g == 0) ? t : cmul(wr0, t);
+                        const float2 wkm = (g == 0) ? tm : cmul(wr1, tm);
+                        const float ex = 0.5f * (A.x + Bq.x), ey = 0.5f * (A.y - Bq.y);
+                        const float dx = 0.5f * (A.x - Bq.x), dy = 0.5f * (A.y + Bq.y);
+                        const float2 X = make_float2(ex + wk.x * dy + wk.y * dx, ey + wk.y * dy - wk.x * dx);
+                        const float2 Xm = make_float2(ex + wkm.x * dy - wkm.y * dx, -ey + wkm.y * dy + wkm.x * dx);
+                        if (k < sp.fcount) {
+                            const bool pk = phase && (k < sp.klo || k > sp.khi);
+                            const float e = pk ? energy_phase(X, efac(k), k >= sp.khf ? cmul(rot, hrot) : rot, Kc)
+                                               : Kc * (X.x * X.x + X.y * X.y);
+                            sink.put(k, e);
+                        }
+                        if (km < sp.fcount) {
+                            const bool pk = phase && (km < sp.klo || km > sp.khi);
+                            float e;
+                            if (pk) {
+                                const float2 rotm = cmulc(ew, rot);  // e^{i 2 pi c} conj(rot)
+                                e = energy_phase(Xm, efac(km), km >= sp.khf ? cmul(rotm, hrot) : rotm, Kc);
+                            } else {
+                                e = Kc * (Xm.x * Xm.x + Xm.y * Xm.y);
+                            }
+                            sink.put(km, e);
+                        }
+                        if (phase) rot = cmul(rot, step);
+                        t = tn;
+                    }
+                    if (g == 0 && tau == TPW - 1) {
+                        // q = L/2, its own mirror; t = W_2L^{L/2}
+                        const int q = L / 2;
+                        const int k = M * q;
+                        const float2 A = buf[pad16(o0 + q)];
+                        const float ex = A.x, dy = A.y;
+                        const float2 X = make_float2(ex + t.x * dy, t.y * dy);
+                        if (k < sp.fcount) {
+                            const bool pk = k < sp.klo || k > sp.khi;
+                            float e;
+                            if (pk) {
+                                const float2 rk = centre_rot((unsigned)k, m.z, cf, nfu, tw);
+                                const float4 hr = s_rot[w];
+                                e = energy_phase(X, efac(k), k >= sp.khf ? cmul(rk, make_float2(hr.x, hr.y)) : rk, Kc);
+                            } else {
+                                e = Kc * (X.x * X.x + X.y * X.y);
+                            }
+                            sink.put(k, e);
+                        }
+                    }
+                }
+                if (!COLLECT) sink_reduce<TPW>(sink.best, s_key, w, valid, tid);
+            }
+        } else if constexpr (!kSplit) {
             for (int base = 0; base < ntasks; base += T) {
                 const int task = base + tid;
                 const bool valid = task < ntasks;
