@@ -589,6 +589,58 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
             // CH - 1 of one window; the tasks holding phase-dependent bins (k < klo
             // or k > khi) are the first tlo and those from thi on, the same in every
             // window, and only their phase-dependent bins are left to (3b).
+            if constexpr (MODE == MODE_SINGLE) {
+                // bins k and Nh - k from one pair of loads, as at L = 4096 (the
+                // phase-dependent ones, whichever task holds them, are (3b)'s)
+                constexpr int QH = CH / 2;
+                for (int base = 0; base < ntasks; base += T) {
+                    const int task = base + tid;
+                    const bool valid = task < ntasks;
+                    const int w = valid ? task / TPW : 0;
+                    const int tau = task - w * TPW;
+                    BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
+                    if (valid) {
+                        const int nq = pair ? CH : QH;
+                        const int q0 = tau * nq;
+                        const int o0 = (w * nf) << LOGL;
+                        const int ob = pair ? o0 + L : o0;
+                        float2 t = __ldg(tw + (q0 << (12 - LOGL)));  // W_2L^q
+#pragma unroll 2
+                        for (int qq = 0; qq < nq; ++qq) {
+                            const int q = q0 + qq;
+                            const int k = M * q + rho0;
+                            const int km = Nh - k;
+                            const float2 A = buf[pad16(o0 + q)];
+                            const float2 Bq = (g == 0) ? buf[pad16(o0 + ((L - q) & (L - 1)))] : buf[pad16(ob + L - 1 - q)];
+                            const float2 tn = cmul(t, make_float2(kW2L[LOGL].x, kW2L[LOGL].y));
+                            const float2 tm = (g == 0) ? make_float2(-t.x, t.y) : make_float2(-tn.x, tn.y);
+                            const float2 wk = (g == 0) ? t : cmul(wr0, t);
+                            const float2 wkm = (g == 0) ? tm : cmul(wr1, tm);
+                            const float ex = 0.5f * (A.x + Bq.x), ey = 0.5f * (A.y - Bq.y);
+                            const float dx = 0.5f * (A.x - Bq.x), dy = 0.5f * (A.y + Bq.y);
+                            if (k < sp.fcount && k >= sp.klo && k <= sp.khi) {
+                                const float2 X = make_float2(ex + wk.x * dy + wk.y * dx, ey + wk.y * dy - wk.x * dx);
+                                sink.put(k, Kc * (X.x * X.x + X.y * X.y));
+                            }
+                            if (km < sp.fcount && km >= sp.klo && km <= sp.khi) {
+                                const float2 Xm = make_float2(ex + wkm.x * dy - wkm.y * dx, -ey + wkm.y * dy + wkm.x * dx);
+                                sink.put(km, Kc * (Xm.x * Xm.x + Xm.y * Xm.y));
+                            }
+                            t = tn;
+                        }
+                        if (g == 0 && tau == TPW - 1) {
+                            // q = L/2, its own mirror; t = W_2L^{L/2}
+                            const int k = M * (L / 2);
+                            if (k < sp.fcount && k >= sp.klo && k <= sp.khi) {
+                                const float2 A = buf[pad16(o0 + L / 2)];
+                                const float2 X = make_float2(A.x + t.x * A.y, t.y * A.y);
+                                sink.put(k, Kc * (X.x * X.x + X.y * X.y));
+                            }
+                        }
+                    }
+                    if (!COLLECT) sink_reduce<TPW>(sink.best, s_key, w, valid, tid);
+                }
+            } else
             for (int base = 0; base < ntasks; base += T) {
                 const int task = base + tid;
                 const bool valid = task < ntasks;
