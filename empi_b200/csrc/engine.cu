@@ -266,7 +266,8 @@ struct empi_batch {
 
     BatchDev dev{};
     int refresh_grid = 0, collect_grid = 0, tree_grid = 0, rescore_grid = 0;
-    size_t refresh_smem = 0;
+    size_t refresh_smem = 0;             // the candidate kernel's (largest layout)
+    size_t refresh_smem_lg[kSizes] = {};  // per sub-FFT size
 
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
@@ -312,21 +313,49 @@ void* refresh_kernel_of(int lg) {
 }
 
 template <int MODE>
+size_t refresh_smem_of(int lg) {
+    switch (lg) {
+        case 0: return refresh_smem_bytes<MODE, 0>();
+        case 1: return refresh_smem_bytes<MODE, 1>();
+        case 2: return refresh_smem_bytes<MODE, 2>();
+        case 3: return refresh_smem_bytes<MODE, 3>();
+        case 4: return refresh_smem_bytes<MODE, 4>();
+        case 5: return refresh_smem_bytes<MODE, 5>();
+        case 6: return refresh_smem_bytes<MODE, 6>();
+        case 7: return refresh_smem_bytes<MODE, 7>();
+        case 8: return refresh_smem_bytes<MODE, 8>();
+        case 9: return refresh_smem_bytes<MODE, 9>();
+        case 10: return refresh_smem_bytes<MODE, 10>();
+        case 11: return refresh_smem_bytes<MODE, 11>();
+        default: return refresh_smem_bytes<MODE, 12>();
+    }
+}
+
+template <int MODE>
 empi_status configure_refresh(empi_batch* b) {
-    const size_t smem = refresh_smem_bytes<MODE>();
     int occ = 1 << 30;
+    size_t most = 0;
     for (int lg : b->sizes) {
         void* fn = refresh_kernel_of<MODE>(lg);
+        const size_t smem = refresh_smem_of<MODE>(lg);
         CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        {
+            // as much L1 as two CTAs' shared memory leaves (percent of the maximum carveout)
+            const int pct = (int)std::min<size_t>(100, (2 * (smem + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024));
+            CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+        }
         int o = 0;
         CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fn, kUnitThreads, smem));
         occ = std::min(occ, o);
         b->refresh_fn[lg] = fn;
+        b->refresh_smem_lg[lg] = smem;
     }
+    // the candidate path runs any size in one kernel: the largest layout
+    for (int lg = 0; lg < kSizes; ++lg) most = std::max(most, refresh_smem_of<MODE>(lg));
     b->collect_fn = (void*)k_collect<MODE>;
-    CUDA_TRY(cudaFuncSetAttribute(b->collect_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_TRY(cudaFuncSetAttribute(b->collect_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most));
     if (occ < 1 || occ == (1 << 30)) return fail(EMPI_ERR_INTERNAL, "refreshKernelDoesNotFit");
-    b->refresh_smem = smem;
+    b->refresh_smem = most;
     b->refresh_grid = b->eng->sms * occ;
     b->collect_grid = b->eng->sms;
     return EMPI_OK;
@@ -345,14 +374,15 @@ void launch_refresh(empi_batch* b, cudaStream_t s) {
     empi_engine* e = b->eng;
     void* args[] = {&b->dev};
     if (b->sizes.size() == 1) {
-        cudaLaunchKernel(b->refresh_fn[b->sizes[0]], dim3(b->refresh_grid), dim3(kUnitThreads), args, b->refresh_smem, s);
+        cudaLaunchKernel(b->refresh_fn[b->sizes[0]], dim3(b->refresh_grid), dim3(kUnitThreads), args,
+                         b->refresh_smem_lg[b->sizes[0]], s);
         return;
     }
     cudaEventRecord(e->fork, s);
     for (size_t i = 0; i < b->sizes.size(); ++i) {
         cudaStreamWaitEvent(e->aux[i], e->fork, 0);
         cudaLaunchKernel(b->refresh_fn[b->sizes[i]], dim3(b->refresh_grid), dim3(kUnitThreads), args,
-                         b->refresh_smem, e->aux[i]);
+                         b->refresh_smem_lg[b->sizes[i]], e->aux[i]);
         cudaEventRecord(e->join[i], e->aux[i]);
     }
     for (size_t i = 0; i < b->sizes.size(); ++i) cudaStreamWaitEvent(s, e->join[i], 0);

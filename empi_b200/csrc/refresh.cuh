@@ -17,7 +17,6 @@
 
 constexpr int kVPT = kUnitPoints / kUnitThreads;
 constexpr int kBufFloat2 = kUnitPoints + kUnitPoints / 16 + 16;
-constexpr int kAccBins = kUnitPoints + kMaxWindowsPerUnit;
 constexpr int kBinsPerTask = 8;  // consecutive q per thread in the spectrum stage
 constexpr int kEtabSmem = 512;   // expFactor entries of one scale staged in shared memory
 
@@ -43,19 +42,26 @@ constexpr Rot kW2L[14] = {
     {0.99999992646571785f, -0.00038349518757139556f},
 };
 
-// shared-memory layout of a refresh CTA
+// shared-memory layout of a refresh CTA for sub-FFT size 2^LOGL: the window
+// tables hold at most NW windows (a unit of kUnitPoints points holds
+// kUnitPoints / L windows), so large transforms leave the rest of the SM's
+// on-chip memory to the L1 cache that serves the residual loads
+template <int LOGL>
 struct RefreshSmem {
+    static constexpr int NW = (kUnitPoints >> LOGL) < kMaxWindowsPerUnit ? (kUnitPoints >> LOGL) : kMaxWindowsPerUnit;
     static constexpr size_t buf = 0;
-    static constexpr size_t win = buf + sizeof(float2) * kBufFloat2;          // int4 (iL, W, ci, cf bits)
-    static constexpr size_t rot = win + sizeof(int4) * kMaxWindowsPerUnit;    // float4 (hrot, step)
-    static constexpr size_t key = rot + sizeof(float4) * kMaxWindowsPerUnit;  // u32 energy bits
-    static constexpr size_t etab = key + sizeof(unsigned) * kMaxWindowsPerUnit;  // float, kEtabSmem
-    static constexpr size_t acc = etab + sizeof(float) * kEtabSmem;
+    static constexpr size_t win = buf + sizeof(float2) * kBufFloat2;  // int4 (iL, W, ci, cf bits)
+    static constexpr size_t rot = win + sizeof(int4) * NW;            // float4 (hrot, step)
+    static constexpr size_t key = rot + sizeof(float4) * NW;          // u32 energy bits
+    static constexpr size_t etab = key + sizeof(unsigned) * NW;       // float, kEtabSmem
+    static constexpr size_t acc = etab + sizeof(float) * kEtabSmem;   // (MMP) per-bin channel sums
 };
 
-template <int MODE>
+template <int MODE, int LOGL>
 constexpr size_t refresh_smem_bytes() {
-    return RefreshSmem::acc + (MODE == MODE_SINGLE ? 0 : sizeof(float) * kAccBins * (MODE == MODE_MMP1 ? 3 : 1));
+    return RefreshSmem<LOGL>::acc + (MODE == MODE_SINGLE ? 0
+                                                       : sizeof(float) * (kUnitPoints + RefreshSmem<LOGL>::NW) *
+                                                             (MODE == MODE_MMP1 ? 3 : 1));
 }
 
 // e^{i psi} with psi = 2 theta_kk = 2 pi (2 kk c / Nfft), c = ci + cf the
@@ -155,12 +161,12 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
     constexpr int L = 1 << LOGL;
     constexpr int CH = L < kBinsPerTask ? L : kBinsPerTask;  // q values per task
     constexpr int TPW = L / CH;                                // tasks per window
-    float2* buf = reinterpret_cast<float2*>(smem + RefreshSmem::buf);
-    int4* s_win = reinterpret_cast<int4*>(smem + RefreshSmem::win);
-    float4* s_rot = reinterpret_cast<float4*>(smem + RefreshSmem::rot);
-    float* s_etab = reinterpret_cast<float*>(smem + RefreshSmem::etab);
-    unsigned* s_key = reinterpret_cast<unsigned*>(smem + RefreshSmem::key);
-    float* acc = reinterpret_cast<float*>(smem + RefreshSmem::acc);
+    float2* buf = reinterpret_cast<float2*>(smem + RefreshSmem<LOGL>::buf);
+    int4* s_win = reinterpret_cast<int4*>(smem + RefreshSmem<LOGL>::win);
+    float4* s_rot = reinterpret_cast<float4*>(smem + RefreshSmem<LOGL>::rot);
+    float* s_etab = reinterpret_cast<float*>(smem + RefreshSmem<LOGL>::etab);
+    unsigned* s_key = reinterpret_cast<unsigned*>(smem + RefreshSmem<LOGL>::key);
+    float* acc = reinterpret_cast<float*>(smem + RefreshSmem<LOGL>::acc);
 
     const InstPlan ip = b.insts[inst];
     const DictPlan dp = b.dicts[ip.dict];
