@@ -376,8 +376,8 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
         // faster; MMP1 folds the phase into its channel sums.  Those keep the
         // single pass.
         constexpr bool kSplit = MODE != MODE_MMP1 && LOGL >= 6 && LOGL <= 11;
-        if constexpr (!kSplit && LOGL == 12 && MODE == MODE_SINGLE) {
-            // Mirrored pairs: bins k and Nh - k read the same two values
+        if constexpr (!kSplit && (LOGL == 12 || (LOGL >= 3 && LOGL <= 5)) && MODE == MODE_SINGLE) {
+            // (L = 4096 and 8 <= L <= 32.)  Mirrored pairs: bins k and Nh - k read the same two values
             // (Z[k], Z[Nh - k]) with A and B exchanged, so one pair of loads
             // gives both.  A task takes q0 .. q0 + nq - 1 and their mirrors: the
             // partner residue's L - 1 - q (pairs, g = 1) or L - q (g = 0, where
