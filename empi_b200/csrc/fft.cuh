@@ -95,8 +95,15 @@ __device__ __forceinline__ void fft_pass(float2* buf, int logL, int logNs, int p
         if (job < jobs) {
             const int j = job & (Q - 1);
             const int base = (job >> logQ) << logL;
+            if (Q % 16 == 0) {
+                // stride Q a multiple of 16: the padding adds Q / 16 per step
+                const float2* src = buf + pad16(base + j);
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[jj][r] = buf[pad16(base + j + r * Q)];
+                for (int r = 0; r < R; ++r) v[jj][r] = src[r * (Q + (Q >> 4))];
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[jj][r] = buf[pad16(base + j + r * Q)];
+            }
             const int k = j & (Ns - 1);
             if (Ns > 1) {
                 // W^(k r) by repeated multiplication with W^k from the table:
@@ -121,8 +128,11 @@ __device__ __forceinline__ void fft_pass(float2* buf, int logL, int logNs, int p
             const int j = job & (Q - 1);
             const int k = j & (Ns - 1);
             const int ob = ((job >> logQ) << logL) + (j - k) * R + k;
+            // ob mod 16 plus any step r Ns mod 16 stays below 16, so the padding
+            // of ob + r Ns is that of ob plus (r Ns) / 16
+            float2* dst = buf + pad16(ob);
 #pragma unroll
-            for (int r = 0; r < R; ++r) buf[pad16(ob + r * Ns)] = v[jj][r];
+            for (int r = 0; r < R; ++r) dst[r * Ns + ((r * Ns) >> 4)] = v[jj][r];
         }
     }
     __syncthreads();
