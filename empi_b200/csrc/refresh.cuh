@@ -321,14 +321,15 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                         pf = cmul(pf, jpstep);
                     }
                 }
-                const int o = ((w * nf) << LOGL) + jq * R0;
+                // o mod 16 is a multiple of R0, so o + rr keeps o's padding
+                float2* po = buf + pad16(((w * nf) << LOGL) + jq * R0);
                 dft<R0>(v1);
 #pragma unroll
-                for (int rr = 0; rr < R0; ++rr) buf[pad16(o + rr)] = v1[rr];
+                for (int rr = 0; rr < R0; ++rr) po[rr] = v1[rr];
                 if (pair) {
                     dft<R0>(v2);
 #pragma unroll
-                    for (int rr = 0; rr < R0; ++rr) buf[pad16(o + L + rr)] = v2[rr];
+                    for (int rr = 0; rr < R0; ++rr) po[L + L / 16 + rr] = v2[rr];
                 }
             }
             __syncthreads();
@@ -340,14 +341,15 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                 for (int w = 0; w < nwin; ++w) {
                     const int4 m = s_win[w];
                     const float cf = __int_as_float(m.w);
-                    const int o = (w * nf) << LOGL;
+                    // points np0 + i T: padded offsets step by T + T / 16
+                    float2* pp = buf + pad16(((w * nf) << LOGL) + np0);
                     float2 t = t0, pf = p0;
 #pragma unroll 2
-                    for (int np = np0; np < L; np += kUnitThreads) {
+                    for (int np = np0; np < L; np += kUnitThreads, pp += kUnitThreads + kUnitThreads / 16) {
                         float2 a1, a2;
                         load_point(m, cf, np, t, a1, a2);
-                        buf[pad16(o + np)] = a1;
-                        if (pair) buf[pad16(o + L + np)] = cmul(a2, pf);
+                        pp[0] = a1;
+                        if (pair) pp[L + L / 16] = cmul(a2, pf);
                         t = cmul(t, tstep);
                         pf = cmul(pf, pstep);
                     }
@@ -409,14 +411,17 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     }
                     const int o0 = (w * nf) << LOGL;
                     const int ob = pair ? o0 + L : o0;  // the partner residue's FFT
+                    // q0 .. q0 + nq - 1 and L - 1 - q stay inside one 16-block each
+                    const float2* pA = buf + pad16(o0 + q0);
+                    const float2* pB = buf + pad16(ob + L - 1 - q0);
                     float2 t = __ldg(tw + (q0 << (12 - LOGL)));  // W_2L^q
 #pragma unroll 2
                     for (int qq = 0; qq < nq; ++qq) {
                         const int q = q0 + qq;
                         const int k = M * q + rho0;
                         const int km = Nh - k;
-                        const float2 A = buf[pad16(o0 + q)];
-                        const float2 Bq = (g == 0) ? buf[pad16(o0 + ((L - q) & (L - 1)))] : buf[pad16(ob + L - 1 - q)];
+                        const float2 A = pA[qq];
+                        const float2 Bq = (g == 0) ? buf[pad16(o0 + ((L - q) & (L - 1)))] : pB[-qq];
                         const float2 tn = cmul(t, make_float2(kW2L[LOGL].x, kW2L[LOGL].y));  // W_2L^{q+1}
                         // W_2L^{L-q} = -conj(W_2L^q); W_2L^{L-1-q} = -conj(W_2L^{q+1})
                         const float2 tm = (g == 0) ? make_float2(-t.x, t.y) : make_float2(-tn.x, tn.y);
@@ -610,14 +615,16 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                         const int q0 = tau * nq;
                         const int o0 = (w * nf) << LOGL;
                         const int ob = pair ? o0 + L : o0;
+                        const float2* pA = buf + pad16(o0 + q0);
+                        const float2* pB = buf + pad16(ob + L - 1 - q0);
                         float2 t = __ldg(tw + (q0 << (12 - LOGL)));  // W_2L^q
 #pragma unroll 2
                         for (int qq = 0; qq < nq; ++qq) {
                             const int q = q0 + qq;
                             const int k = M * q + rho0;
                             const int km = Nh - k;
-                            const float2 A = buf[pad16(o0 + q)];
-                            const float2 Bq = (g == 0) ? buf[pad16(o0 + ((L - q) & (L - 1)))] : buf[pad16(ob + L - 1 - q)];
+                            const float2 A = pA[qq];
+                            const float2 Bq = (g == 0) ? buf[pad16(o0 + ((L - q) & (L - 1)))] : pB[-qq];
                             const float2 tn = cmul(t, make_float2(kW2L[LOGL].x, kW2L[LOGL].y));
                             const float2 tm = (g == 0) ? make_float2(-t.x, t.y) : make_float2(-tn.x, tn.y);
                             const float2 wk = (g == 0) ? t : cmul(wr0, t);
