@@ -246,6 +246,7 @@ __global__ void k_sched_a(BatchDev b, int mode, int only_scale, double tA_in, do
     __syncthreads();
     int* units = b.ij_units + ip.ij_off + inst;
     int* chunks = b.ij_chunks + ip.ij_off + inst;
+    double st_flops = 0.0, st_bytes = 0.0, st_slots = 0.0;  // statistics, one atomic each per CTA
     for (int j = threadIdx.x; j < dp.nscales; j += blockDim.x) {
         const ScalePlan sp = b.scales[dp.scale0 + j];
         int lo = 0, hi = -1;
@@ -285,13 +286,33 @@ __global__ void k_sched_a(BatchDev b, int mode, int only_scale, double tA_in, do
             window_bounds(grid_t(lo, dp.tMax, sp.tcount), sp.hw, dp.fs, dp.N, iL0, iR0, tf);
             window_bounds(grid_t(hi, dp.tMax, sp.tcount), sp.hw, dp.fs, dp.N, iL1, iR1, tf);
             const double lg = log2((double)sp.nfft);
-            atomicAdd(b.stats + 0, (double)n * ip.C * 2.5 * sp.nfft * lg);
-            atomicAdd(b.stats + 1, 4.0 * ip.C * (double)(iR1 - iL0 + 1) + 8.0 * (double)n * sp.G);
-            atomicAdd(b.stats + 2, (double)n * sp.G);
+            st_flops += (double)n * ip.C * 2.5 * sp.nfft * lg;
+            st_bytes += 4.0 * ip.C * (double)(iR1 - iL0 + 1) + 8.0 * (double)n * sp.G;
+            st_slots += (double)n * sp.G;
         }
         units[j + 1] = nu;
         chunks[j + 1] = nc;
         b.ij_crange[ip.ij_off + j] = make_int2(c0, nc);
+    }
+    {
+        __shared__ double s_st[3][32];
+#pragma unroll
+        for (int off = 16; off; off >>= 1) {
+            st_flops += __shfl_down_sync(0xffffffffu, st_flops, off);
+            st_bytes += __shfl_down_sync(0xffffffffu, st_bytes, off);
+            st_slots += __shfl_down_sync(0xffffffffu, st_slots, off);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            s_st[0][threadIdx.x >> 5] = st_flops;
+            s_st[1][threadIdx.x >> 5] = st_bytes;
+            s_st[2][threadIdx.x >> 5] = st_slots;
+        }
+        __syncthreads();
+        if (threadIdx.x < 3) {
+            double v = 0.0;
+            for (int wp = 0; wp < (int)(blockDim.x >> 5); ++wp) v += s_st[threadIdx.x][wp];
+            if (v != 0.0) atomicAdd(b.stats + threadIdx.x, v);
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -364,11 +385,9 @@ __global__ void k_sched_b(BatchDev b) {
 __global__ void k_tree(BatchDev b) {
     const int lane = threadIdx.x & 31;
     const int total = b.ctr[CTR_TOTAL_CHUNKS];
-    for (;;) {
-        int item = 0;
-        if (lane == 0) item = atomicAdd(b.ctr + CTR_TREE, 1);
-        item = __shfl_sync(0xffffffffu, item, 0);
-        if (item >= total) break;
+    // a fixed chunk per warp and stride: no work-queue atomic per chunk
+    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int item = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); item < total; item += nwarps) {
         const int inst = upper_index(b.inst_chunks, b.ninst, item);
         int rem = item - b.inst_chunks[inst];
         const InstPlan ip = b.insts[inst];
