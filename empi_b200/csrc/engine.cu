@@ -400,7 +400,7 @@ void launch_update(empi_batch* b, int sched_mode, int only_scale, double tA, dou
     const int ninst = (int)b->insts.size();
     cudaMemsetAsync(b->dev.lcount, 0, sizeof(int) * 2 * 16, s);  // lcount and lhead
     k_sched_a<<<ninst, 128, 0, s>>>(b->dev, sched_mode, only_scale, tA, sA);
-    k_sched_b<<<1, 1024, 0, s>>>(b->dev);
+    k_sched_b<<<1, std::min(1024, 32 * ((ninst + 31) / 32)), 0, s>>>(b->dev);
     if (e0) cudaEventRecord(e0, s);
     launch_refresh(b, s);
     if (e1) cudaEventRecord(e1, s);
@@ -413,13 +413,13 @@ void launch_select(empi_batch* b, cudaStream_t s) {
     const int ninst = (int)b->insts.size();
     k_cand_slots<<<ninst, 256, 0, s>>>(b->dev);
     launch_collect(b, s);
-    k_rescore<<<b->rescore_grid, 128, 0, s>>>(b->dev);
+    k_rescore<<<b->rescore_grid, 512, 0, s>>>(b->dev);
     k_select<<<ninst, 128, 0, s>>>(b->dev);
 }
 
 void launch_iteration(empi_batch* b, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
     launch_select(b, s);
-    k_subtract<<<(int)b->blk_ic.size(), 256, 0, s>>>(b->dev);
+    k_subtract<<<(int)b->blk_ic.size(), 1024, 0, s>>>(b->dev);
     launch_update(b, SCHED_ITERATE, -1, 0.0, 0.0, s, e0, e1);
 }
 
@@ -641,7 +641,7 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
     st = configure(b.get());
     if (st != EMPI_OK) return st;
     b->tree_grid = eng->sms * 8;
-    b->rescore_grid = eng->sms * 4;
+    b->rescore_grid = eng->sms;
     if (b->max_n * sizeof(double) > 48 * 1024 && !b->fit_map.empty()) {
         CUDA_TRY(cudaFuncSetAttribute(k_mmp2_fit, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)(b->max_n * sizeof(double))));
