@@ -791,9 +791,10 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
     __syncthreads();
 }
 
-// Out-of-line instance of one size, for the candidate path's runtime dispatch.
+// One size of the candidate path's runtime dispatch (inlined: the call
+// boundary of an out-of-line body cost more than the larger kernel).
 template <int LOGL, int MODE>
-__device__ __noinline__ void collect_body(const BatchDev& b, unsigned char* smem, int inst, int j, int g, int t,
+__device__ __forceinline__ void collect_body(const BatchDev& b, unsigned char* smem, int inst, int j, int g, int t,
                                           unsigned thr_bits) {
     unit_body<LOGL, MODE, true>(b, smem, inst, j, g, t, 1, thr_bits);
 }
