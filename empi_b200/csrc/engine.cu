@@ -405,7 +405,6 @@ void launch_update(empi_batch* b, int sched_mode, int only_scale, double tA, dou
     launch_refresh(b, s);
     if (e1) cudaEventRecord(e1, s);
     k_tree<<<b->tree_grid, 256, 0, s>>>(b->dev);
-    k_root<<<ninst, 256, 0, s>>>(b->dev);
 }
 
 // candidates -> FP64 rescore -> atom
@@ -530,8 +529,8 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
         lsum += lcapl[l];
     }
     // kernels per MP iteration: k_cand_slots, k_collect, k_rescore, k_select,
-    // k_subtract, k_sched_a/b, one refresh per size, k_tree, k_root
-    b->launches_per_iter = 9 + (int)b->sizes.size();
+    // k_subtract, k_sched_a/b, one refresh per size, k_tree
+    b->launches_per_iter = 8 + (int)b->sizes.size();
     if (lsum > (1LL << 31) - 1) return fail(EMPI_ERR_SIGNAL_TOO_LONG, "batchTooLarge");
     const int band_cap = eng->opts.candidate_capacity > 0 ? eng->opts.candidate_capacity
                                                           : std::max(8192, 64 * ninst);
@@ -751,7 +750,7 @@ extern "C" empi_status empi_batch_run(empi_batch* b) {
     CUDA_TRY(cudaEventRecord(b->run_start, s));
     k_init<<<(int)b->blk_ic.size(), 256, 0, s>>>(b->dev, 1);
     launch_update(b, SCHED_INIT, -1, 0.0, 0.0, s, timing ? b->ev[0] : nullptr, timing ? b->ev[1] : nullptr);
-    int launches = 5 + (int)b->sizes.size();  // k_init, k_sched_a/b, refreshes, k_tree, k_root
+    int launches = 4 + (int)b->sizes.size();  // k_init, k_sched_a/b, refreshes, k_tree
     double refresh_ms = 0.0;
     int refresh_launches = 0;
     if (timing) {

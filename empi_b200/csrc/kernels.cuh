@@ -1,8 +1,8 @@
 // sm_100a kernels of the Matching Pursuit loop.
 //
 // Per MP iteration the device runs (all launches captured in a CUDA graph):
-//   k_cand_slots  slots whose FP32 max lies within the candidate band of the
-//                 instance's best (reads the tournament tree top-down)
+//   k_cand_slots  the instance's best over its chunk maxima (the tree's root),
+//                 then the slots whose FP32 max lies within the candidate band
 //   k_refresh<COLLECT>  FP32 recompute of those slots, emitting every bin in
 //                 the band
 //   k_rescore     FP64 direct DFT of each candidate bin, per channel
@@ -11,7 +11,6 @@
 //   k_sched_a/b   stop test, dirty t-range per scale, work-unit prefix sums
 //   k_refresh     windowed FFT + energies + per-slot max over the dirty range
 //   k_tree        leaf-chunk maxima for the chunks the refresh touched
-//   k_root        per-instance maximum over chunk maxima
 // Waits are never spun on: ordering comes from kernel boundaries only.
 #pragma once
 
@@ -433,22 +432,6 @@ __device__ __forceinline__ unsigned long long block_max_u64(unsigned long long v
     return v;
 }
 
-// Root: per-instance best over chunk maxima.
-__global__ void k_root(BatchDev b) {
-    __shared__ unsigned long long red[32];
-    const int inst = blockIdx.x;
-    if (b.state[inst].status != ST_RUNNING) return;
-    const InstPlan ip = b.insts[inst];
-    const DictPlan dp = b.dicts[ip.dict];
-    unsigned long long best = 0;
-    for (int c = threadIdx.x; c < dp.chunks; c += blockDim.x) {
-        const unsigned long long v = b.chunks[ip.chunk_off + c];
-        best = v > best ? v : best;
-    }
-    best = block_max_u64(best, red);
-    if (threadIdx.x == 0) b.state[inst].best32 = best;
-}
-
 // ------------------------------------------------------------ candidates
 
 __device__ __forceinline__ void slot_to_jtg(const BatchDev& b, const DictPlan& dp, long long slot, int& j, int& t,
@@ -466,18 +449,31 @@ __device__ __forceinline__ void slot_to_jtg(const BatchDev& b, const DictPlan& d
     g = (int)(rel - (long long)t * sp.G);
 }
 
-// One CTA per instance: every slot whose FP32 max is within the band of the
-// instance's best becomes a candidate (qualifying chunks first, then their
-// slots).
+// One CTA per instance: the root of the tournament tree (the instance's best
+// over its chunk maxima), then every slot whose FP32 max is within the band of
+// it becomes a candidate (qualifying chunks first, then their slots).
 __global__ void k_cand_slots(BatchDev b) {
     __shared__ int s_chunks[256];
     __shared__ int s_n;
+    __shared__ unsigned long long red[32];
     const int inst = blockIdx.x;
     InstState& st = b.state[inst];
     if (st.status != ST_RUNNING) return;
     const InstPlan ip = b.insts[inst];
     const DictPlan dp = b.dicts[ip.dict];
-    const unsigned best = (unsigned)(st.best32 >> 32);
+    unsigned long long root = 0;
+    for (int c = threadIdx.x; c < dp.chunks; c += blockDim.x) {
+        const unsigned long long v = b.chunks[ip.chunk_off + c];
+        root = v > root ? v : root;
+    }
+    root = block_max_u64(root, red);  // valid in thread 0
+    __shared__ unsigned long long s_root;
+    if (threadIdx.x == 0) {
+        st.best32 = root;
+        s_root = root;
+    }
+    __syncthreads();
+    const unsigned best = (unsigned)(s_root >> 32);
     if (best == 0u) {  // nothing beats 0: src/gabor.cpp:108-110
         if (threadIdx.x == 0) {
             st.status = ST_ERROR;
