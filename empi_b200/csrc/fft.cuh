@@ -138,30 +138,10 @@ __device__ __forceinline__ void fft_pass(float2* buf, int logL, int logNs, int p
     __syncthreads();
 }
 
-// Forward FFT of size L = 2^logL on `points` consecutive values (a batch of
-// points / L transforms) held padded in buf.  Starts and ends with the data in
-// shared memory; callers synchronise before the call.
-template <int VPT, int TW_N>
-__device__ __forceinline__ void fft_batch(float2* buf, int logL, int points, const float2* __restrict__ tw) {
-    int logNs = 0;
-    const int first = logL & 3;
-    if (first == 1) {
-        fft_pass<2, VPT, TW_N>(buf, logL, logNs, points, tw);
-        logNs += 1;
-    } else if (first == 2) {
-        fft_pass<4, VPT, TW_N>(buf, logL, logNs, points, tw);
-        logNs += 2;
-    } else if (first == 3) {
-        fft_pass<8, VPT, TW_N>(buf, logL, logNs, points, tw);
-        logNs += 3;
-    }
-    while (logNs < logL) {
-        fft_pass<16, VPT, TW_N>(buf, logL, logNs, points, tw);
-        logNs += 4;
-    }
-}
-
-// Same as fft_batch with the size fixed at compile time.
+// Forward FFT of size L = 2^LOGL on `points` consecutive values (a batch of
+// points / L transforms) held padded in buf: the odd radix (2, 4 or 8) first,
+// then radix-16 passes.  Starts and ends with the data in shared memory;
+// callers synchronise before the call.
 template <int VPT, int TW_N, int LOGL>
 __device__ __forceinline__ void fft_batch_t(float2* buf, int points, const float2* __restrict__ tw) {
     constexpr int first = LOGL & 3;
