@@ -372,12 +372,11 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
         }
         // (3) spectrum, energies, maxima
         const bool last = (c == ip.C - 1);
-        // Two passes (3a, 3b) for 64 <= L <= 2048.  Small transforms (L <= 32)
-        // are almost all phase-dependent bins; at L = 4096 a unit holds one or two
-        // windows, too few phase tasks to spread, and the single pass measured
-        // faster; MMP1 folds the phase into its channel sums.  Those keep the
-        // single pass.
-        constexpr bool kSplit = MODE != MODE_MMP1 && LOGL >= 6 && LOGL <= 11;
+        // Two passes (3a, 3b) for L >= 64 (at L = 4096 the second takes its
+        // bins one per thread).  Small transforms (L <= 32) are almost all
+        // phase-dependent bins, and MMP1 folds the phase into its channel sums:
+        // those keep the single pass.
+        constexpr bool kSplit = MODE != MODE_MMP1 && LOGL >= 6;
         if constexpr (!kSplit && (LOGL == 12 || (LOGL >= 3 && LOGL <= 5)) && MODE == MODE_SINGLE) {
             // (L = 4096 and 8 <= L <= 32.)  Mirrored pairs: bins k and Nh - k read the same two values
             // (Z[k], Z[Nh - k]) with A and B exchanged, so one pair of loads
@@ -698,6 +697,65 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                 }
                 if (!COLLECT && MODE == MODE_SINGLE) sink_reduce<TPW>(sink.best, s_key, w, valid, tid);
             }
+            if constexpr (LOGL == 12 && MODE == MODE_SINGLE) {
+                // (3b) at L = 4096: the phase-dependent bins one per thread (a unit
+                // holds one or two windows, so a task-sized item would leave a few
+                // warps doing all of them).  Per half h they are q < ql and
+                // qh <= q < qe (k < klo, k > khi, k < fcount), plus the Nyquist bin.
+                int ql[2] = {0, 0}, qh[2] = {0, 0}, cnt[2] = {0, 0};
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    if (h < nf) {
+                        const int rho = h ? rho1 : rho0;
+                        const int qe = max(0, min(L, (sp.fcount - rho + M - 1) / M));
+                        const int lo = sp.klo - rho;
+                        ql[h] = min(qe, lo > 0 ? (lo + M - 1) / M : 0);
+                        const int hi = sp.khi - rho;
+                        qh[h] = max(ql[h], min(qe, hi >= 0 ? hi / M + 1 : 0));
+                        cnt[h] = ql[h] + (qe - qh[h]);
+                    }
+                }
+                const int nyq = (g == 0 && Nh < sp.fcount) ? 1 : 0;
+                const int nper = cnt[0] + cnt[1] + nyq;
+                for (int i = tid; i < nwin * nper; i += T) {
+                    const int w = i / nper;
+                    int jx = i - w * nper;
+                    const int4 m = s_win[w];
+                    const float cf = __int_as_float(m.w);
+                    const float4 hr = s_rot[w];
+                    const float2 hrot = make_float2(hr.x, hr.y);
+                    const int o0 = (w * nf) << LOGL;
+                    float2 X;
+                    int k;
+                    if (jx == cnt[0] + cnt[1]) {
+                        // Nyquist bin k = Nh (g = 0): X = Re Z[0] - Im Z[0]
+                        const float2 Z0 = buf[pad16(o0)];
+                        X = make_float2(Z0.x - Z0.y, 0.0f);
+                        k = Nh;
+                    } else {
+                        const int h = jx < cnt[0] ? 0 : 1;
+                        if (h) jx -= cnt[0];
+                        const int q = jx < ql[h] ? jx : qh[h] + (jx - ql[h]);
+                        const int rho = h ? rho1 : rho0;
+                        const float2 wr = h ? wr1 : wr0;
+                        const int oa = h ? o0 + L : o0;
+                        const int ob = pair ? (h ? o0 : o0 + L) : o0;
+                        const float2 A = buf[pad16(oa + q)];
+                        const float2 Bq = (g == 0) ? buf[pad16(ob + ((L - q) & (L - 1)))] : buf[pad16(ob + L - 1 - q)];
+                        const float2 t = __ldg(tw + (q << (12 - LOGL)));
+                        const float2 wk = (g == 0) ? t : cmul(wr, t);
+                        const float ex = 0.5f * (A.x + Bq.x), ey = 0.5f * (A.y - Bq.y);
+                        const float dx = 0.5f * (A.x - Bq.x), dy = 0.5f * (A.y + Bq.y);
+                        X = make_float2(ex + wk.x * dy + wk.y * dx, ey + wk.y * dy - wk.x * dx);
+                        k = M * q + rho;
+                    }
+                    const float2 rot = centre_rot((unsigned)k, m.z, cf, nfu, tw);
+                    const float e = energy_phase(X, efac(k), k >= sp.khf ? cmul(rot, hrot) : rot, Kc);
+                    BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
+                    sink.put(k, e);
+                    if (!COLLECT) atomicMax(s_key + w, __float_as_uint(sink.best));
+                }
+            } else
             // (3b) the phase-dependent bins (and the Nyquist bin), task by task as in
             // (3a) but spread over all threads: nph such tasks per window
             for (int i = tid; i < nwin * nph; i += T) {
