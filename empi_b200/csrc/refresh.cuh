@@ -372,8 +372,8 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
         }
         // (3) spectrum, energies, maxima
         const bool last = (c == ip.C - 1);
-        // Two passes (3a, 3b) for L >= 64 (at L = 4096 the second takes its
-        // bins one per thread).  Small transforms (L <= 32) are almost all
+        // Two passes (3a, 3b) for L >= 64 (from L = 1024 on, where a unit holds
+        // at most eight windows, the second takes its bins one per thread).  Small transforms (L <= 32) are almost all
         // phase-dependent bins, and MMP1 folds the phase into its channel sums:
         // those keep the single pass.
         constexpr bool kSplit = MODE != MODE_MMP1 && LOGL >= 6;
@@ -697,10 +697,10 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                 }
                 if (!COLLECT && MODE == MODE_SINGLE) sink_reduce<TPW>(sink.best, s_key, w, valid, tid);
             }
-            if constexpr (LOGL == 12 && MODE == MODE_SINGLE) {
-                // (3b) at L = 4096: the phase-dependent bins one per thread (a unit
-                // holds one or two windows, so a task-sized item would leave a few
-                // warps doing all of them).  Per half h they are q < ql and
+            if constexpr (LOGL >= 10 && MODE == MODE_SINGLE) {
+                // (3b) for L >= 1024: the phase-dependent bins one per thread (a
+                // unit holds at most eight windows, so task-sized items would leave
+                // a few warps doing all of them).  Per half h they are q < ql and
                 // qh <= q < qe (k < klo, k > khi, k < fcount), plus the Nyquist bin.
                 int ql[2] = {0, 0}, qh[2] = {0, 0}, cnt[2] = {0, 0};
 #pragma unroll
