@@ -599,9 +599,10 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
             // CH - 1 of one window; the tasks holding phase-dependent bins (k < klo
             // or k > khi) are the first tlo and those from thi on, the same in every
             // window, and only their phase-dependent bins are left to (3b).
-            if constexpr (MODE == MODE_SINGLE) {
+            if constexpr (MODE == MODE_SINGLE || MODE == MODE_MMP3) {
                 // bins k and Nh - k from one pair of loads, as at L = 4096 (the
-                // phase-dependent ones, whichever task holds them, are (3b)'s)
+                // phase-dependent ones, whichever task holds them, are (3b)'s);
+                // MMP3 adds each channel's energy to the bin's sum instead
                 constexpr int QH = CH / 2;
                 for (int base = 0; base < ntasks; base += T) {
                     const int task = base + tid;
@@ -632,11 +633,15 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                             const float dx = 0.5f * (A.x - Bq.x), dy = 0.5f * (A.y + Bq.y);
                             if (k < sp.fcount && k >= sp.klo && k <= sp.khi) {
                                 const float2 X = make_float2(ex + wk.x * dy + wk.y * dx, ey + wk.y * dy - wk.x * dx);
-                                sink.put(k, Kc * (X.x * X.x + X.y * X.y));
+                                const float e = Kc * (X.x * X.x + X.y * X.y);
+                                if (MODE == MODE_SINGLE) sink.put(k, e);
+                                else acc[w * nb + q] += e;
                             }
                             if (km < sp.fcount && km >= sp.klo && km <= sp.khi) {
                                 const float2 Xm = make_float2(ex + wkm.x * dy - wkm.y * dx, -ey + wkm.y * dy + wkm.x * dx);
-                                sink.put(km, Kc * (Xm.x * Xm.x + Xm.y * Xm.y));
+                                const float e = Kc * (Xm.x * Xm.x + Xm.y * Xm.y);
+                                if (MODE == MODE_SINGLE) sink.put(km, e);
+                                else acc[w * nb + (pair ? 2 * L - 1 - q : (g == 0 ? L - q : L - 1 - q))] += e;
                             }
                             t = tn;
                         }
@@ -646,11 +651,13 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                             if (k < sp.fcount && k >= sp.klo && k <= sp.khi) {
                                 const float2 A = buf[pad16(o0 + L / 2)];
                                 const float2 X = make_float2(A.x + t.x * A.y, t.y * A.y);
-                                sink.put(k, Kc * (X.x * X.x + X.y * X.y));
+                                const float e = Kc * (X.x * X.x + X.y * X.y);
+                                if (MODE == MODE_SINGLE) sink.put(k, e);
+                                else acc[w * nb + L / 2] += e;
                             }
                         }
                     }
-                    if (!COLLECT) sink_reduce<TPW>(sink.best, s_key, w, valid, tid);
+                    if (!COLLECT && MODE == MODE_SINGLE) sink_reduce<TPW>(sink.best, s_key, w, valid, tid);
                 }
             } else
             for (int base = 0; base < ntasks; base += T) {
@@ -697,7 +704,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                 }
                 if (!COLLECT && MODE == MODE_SINGLE) sink_reduce<TPW>(sink.best, s_key, w, valid, tid);
             }
-            if constexpr (LOGL >= 10 && MODE == MODE_SINGLE) {
+            if constexpr (LOGL >= 10 && (MODE == MODE_SINGLE || MODE == MODE_MMP3)) {
                 // (3b) for L >= 1024: the phase-dependent bins one per thread (a
                 // unit holds at most eight windows, so task-sized items would leave
                 // a few warps doing all of them).  Per half h they are q < ql and
@@ -726,12 +733,13 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     const float2 hrot = make_float2(hr.x, hr.y);
                     const int o0 = (w * nf) << LOGL;
                     float2 X;
-                    int k;
+                    int k, aq;
                     if (jx == cnt[0] + cnt[1]) {
                         // Nyquist bin k = Nh (g = 0): X = Re Z[0] - Im Z[0]
                         const float2 Z0 = buf[pad16(o0)];
                         X = make_float2(Z0.x - Z0.y, 0.0f);
                         k = Nh;
+                        aq = L;
                     } else {
                         const int h = jx < cnt[0] ? 0 : 1;
                         if (h) jx -= cnt[0];
@@ -748,12 +756,17 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                         const float dx = 0.5f * (A.x - Bq.x), dy = 0.5f * (A.y + Bq.y);
                         X = make_float2(ex + wk.x * dy + wk.y * dx, ey + wk.y * dy - wk.x * dx);
                         k = M * q + rho;
+                        aq = q + h * L;
                     }
                     const float2 rot = centre_rot((unsigned)k, m.z, cf, nfu, tw);
                     const float e = energy_phase(X, efac(k), k >= sp.khf ? cmul(rot, hrot) : rot, Kc);
-                    BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
-                    sink.put(k, e);
-                    if (!COLLECT) atomicMax(s_key + w, __float_as_uint(sink.best));
+                    if constexpr (MODE == MODE_SINGLE) {
+                        BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
+                        sink.put(k, e);
+                        if (!COLLECT) atomicMax(s_key + w, __float_as_uint(sink.best));
+                    } else {
+                        acc[w * nb + aq] += e;
+                    }
                 }
             } else
             // (3b) the phase-dependent bins (and the Nyquist bin), task by task as in
