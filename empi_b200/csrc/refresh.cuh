@@ -618,7 +618,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                         const float2* pA = buf + pad16(o0 + q0);
                         const float2* pB = buf + pad16(ob + L - 1 - q0);
                         float2 t = __ldg(tw + (q0 << (12 - LOGL)));  // W_2L^q
-#pragma unroll 2
+#pragma unroll 4
                         for (int qq = 0; qq < nq; ++qq) {
                             const int q = q0 + qq;
                             const int k = M * q + rho0;
