@@ -344,7 +344,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     // points np0 + i T: padded offsets step by T + T / 16
                     float2* pp = buf + pad16(((w * nf) << LOGL) + np0);
                     float2 t = t0, pf = p0;
-#pragma unroll 2
+#pragma unroll 4
                     for (int np = np0; np < L; np += kUnitThreads, pp += kUnitThreads + kUnitThreads / 16) {
                         float2 a1, a2;
                         load_point(m, cf, np, t, a1, a2);
