@@ -281,6 +281,25 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
             const float* __restrict__ xs = x + m.x;
             a1 = make_float2(0.f, 0.f);
             a2 = make_float2(0.f, 0.f);
+            if (F == 1) {
+                // one fold (every scale whose longest window fits its sub-FFT):
+                // no loop and no rotation of the twist to a next fold
+                const int i0 = 2 * np;
+                if (i0 < m.y) {
+                    const float x0 = __ldg(xs + i0);
+                    const float x1 = (i0 + 1 < m.y) ? __ldg(xs + i0 + 1) : 0.0f;
+                    const float d0 = (float)(i0 - m.z) - cf;
+                    const float y0 = d0 * aG2, y1 = (d0 + 1.0f) * aG2;
+                    const float2 z = make_float2(x0 * exp2f(-y0 * y0), x1 * exp2f(-y1 * y1));
+                    if (g == 0) {
+                        a1 = z;
+                    } else {
+                        a1 = cmul(z, t);
+                        if (g >= 2) a2 = cmulc(z, t);
+                    }
+                }
+                return;
+            }
             int n = np;
             for (int mm = 0; mm < F; ++mm, n += L) {
                 const int i0 = 2 * n;
