@@ -432,7 +432,12 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     // q0 .. q0 + nq - 1 and L - 1 - q stay inside one 16-block each
                     const float2* pA = buf + pad16(o0 + q0);
                     const float2* pB = buf + pad16(ob + L - 1 - q0);
-                    float2 t = __ldg(tw + (q0 << (12 - LOGL)));  // W_2L^q
+                    // W_Nfft^k = W_Nfft^rho0 W_2L^q, rotated by W_2L from bin to bin; the
+                    // mirror's twiddle is -conj(W_Nfft^k) (W_Nfft^M = W_2L and rho1 =
+                    // M - rho0), so with E = (A + conj B) / 2 and D = (A - conj B) / 2i:
+                    // X[k] = E + W D and X[Nh - k] = conj(E - W D)
+                    float2 wk = __ldg(tw + (q0 << (12 - LOGL)));  // W_2L^q
+                    if (g != 0) wk = cmul(wr0, wk);
 #pragma unroll 2
                     for (int qq = 0; qq < nq; ++qq) {
                         const int q = q0 + qq;
@@ -440,15 +445,11 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                         const int km = Nh - k;
                         const float2 A = pA[qq];
                         const float2 Bq = (g == 0) ? buf[pad16(o0 + ((L - q) & (L - 1)))] : pB[-qq];
-                        const float2 tn = cmul(t, make_float2(kW2L[LOGL].x, kW2L[LOGL].y));  // W_2L^{q+1}
-                        // W_2L^{L-q} = -conj(W_2L^q); W_2L^{L-1-q} = -conj(W_2L^{q+1})
-                        const float2 tm = (g == 0) ? make_float2(-t.x, t.y) : make_float2(-tn.x, tn.y);
-                        const float2 wk = (g == 0) ? t : cmul(wr0, t);
-                        const float2 wkm = (g == 0) ? tm : cmul(wr1, tm);
                         const float ex = 0.5f * (A.x + Bq.x), ey = 0.5f * (A.y - Bq.y);
                         const float dx = 0.5f * (A.x - Bq.x), dy = 0.5f * (A.y + Bq.y);
-                        const float2 X = make_float2(ex + wk.x * dy + wk.y * dx, ey + wk.y * dy - wk.x * dx);
-                        const float2 Xm = make_float2(ex + wkm.x * dy - wkm.y * dx, -ey + wkm.y * dy + wkm.x * dx);
+                        const float u = wk.x * dy + wk.y * dx, v = wk.y * dy - wk.x * dx;
+                        const float2 X = make_float2(ex + u, ey + v);
+                        const float2 Xm = make_float2(ex - u, v - ey);
                         if (k < sp.fcount) {
                             const bool pk = phase && (k < sp.klo || k > sp.khi);
                             const float e = pk ? energy_phase(X, efac(k), k >= sp.khf ? cmul(rot, hrot) : rot, Kc)
@@ -467,15 +468,15 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                             sink.put(km, e);
                         }
                         if (phase) rot = cmul(rot, step);
-                        t = tn;
+                        wk = cmul(wk, make_float2(kW2L[LOGL].x, kW2L[LOGL].y));
                     }
                     if (g == 0 && tau == TPW - 1) {
-                        // q = L/2, its own mirror; t = W_2L^{L/2}
+                        // q = L/2, its own mirror; wk = W_2L^{L/2}
                         const int q = L / 2;
                         const int k = M * q;
                         const float2 A = buf[pad16(o0 + q)];
                         const float ex = A.x, dy = A.y;
-                        const float2 X = make_float2(ex + t.x * dy, t.y * dy);
+                        const float2 X = make_float2(ex + wk.x * dy, wk.y * dy);
                         if (k < sp.fcount) {
                             const bool pk = k < sp.klo || k > sp.khi;
                             float e;
@@ -526,16 +527,16 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                         // partner L - 1 - q for g >= 1: a descending run inside one
                         // 16-block, since (L - 1 - q0) mod 16 is 15 or 7
                         const int pb = pad16(ob + L - 1 - q0);
-                        // W_2L^q: the table entry at q0, then one rotation by W_2L per bin
-                        float2 t = __ldg(tw + (q0 << (12 - LOGL)));
+                        // W_Nfft^k = W_Nfft^rho W_2L^q: the table entry at q0, then one
+                        // rotation by W_2L per bin
+                        float2 wk = __ldg(tw + (q0 << (12 - LOGL)));
+                        if (g != 0) wk = cmul(wr, wk);
     #pragma unroll 2
                         for (int qq = 0; qq < CH; ++qq) {
                             const int q = q0 + qq;
                             const int k = M * q + rho;
                             const float2 A = buf[pa + qq];
                             const float2 Bq = (g == 0) ? buf[pad16(ob + ((L - q) & (L - 1)))] : buf[pb - qq];
-                            const float2 wk = (g == 0) ? t : cmul(wr, t);
-                            t = cmul(t, make_float2(kW2L[LOGL].x, kW2L[LOGL].y));
                             const float ex = 0.5f * (A.x + Bq.x), ey = 0.5f * (A.y - Bq.y);
                             const float dx = 0.5f * (A.x - Bq.x), dy = 0.5f * (A.y + Bq.y);
                             const float2 X = make_float2(ex + wk.x * dy + wk.y * dx, ey + wk.y * dy - wk.x * dx);
@@ -556,6 +557,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                                 }
                             }
                             if (phase) rot = cmul(rot, step);
+                            wk = cmul(wk, make_float2(kW2L[LOGL].x, kW2L[LOGL].y));
                         }
                     }
                     if (g == 0 && q0 == 0 && Nh < sp.fcount) {
@@ -618,7 +620,8 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
             // CH - 1 of one window; the tasks holding phase-dependent bins (k < klo
             // or k > khi) are the first tlo and those from thi on, the same in every
             // window, and only their phase-dependent bins are left to (3b).
-            if constexpr (MODE == MODE_SINGLE || MODE == MODE_MMP3) {
+            static_assert(MODE == MODE_SINGLE || MODE == MODE_MMP3, "the split spectrum serves SMP and MMP3");
+            {
                 // bins k and Nh - k from one pair of loads, as at L = 4096 (the
                 // phase-dependent ones, whichever task holds them, are (3b)'s);
                 // MMP3 adds each channel's energy to the bin's sum instead
@@ -636,7 +639,12 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                         const int ob = pair ? o0 + L : o0;
                         const float2* pA = buf + pad16(o0 + q0);
                         const float2* pB = buf + pad16(ob + L - 1 - q0);
-                        float2 t = __ldg(tw + (q0 << (12 - LOGL)));  // W_2L^q
+                        // W_Nfft^k = W_Nfft^rho0 W_2L^q, rotated by W_2L from bin to bin.
+                        // The mirror's twiddle is -conj(W_Nfft^k) (W_Nfft^M = W_2L and
+                        // rho1 = M - rho0), so with E = (A + conj B) / 2 and
+                        // D = (A - conj B) / 2i: X[k] = E + W D, X[Nh-k] = conj(E - W D).
+                        float2 wk = __ldg(tw + (q0 << (12 - LOGL)));  // W_2L^q
+                        if (g != 0) wk = cmul(wr0, wk);
 #pragma unroll 4
                         for (int qq = 0; qq < nq; ++qq) {
                             const int q = q0 + qq;
@@ -644,32 +652,29 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                             const int km = Nh - k;
                             const float2 A = pA[qq];
                             const float2 Bq = (g == 0) ? buf[pad16(o0 + ((L - q) & (L - 1)))] : pB[-qq];
-                            const float2 tn = cmul(t, make_float2(kW2L[LOGL].x, kW2L[LOGL].y));
-                            const float2 tm = (g == 0) ? make_float2(-t.x, t.y) : make_float2(-tn.x, tn.y);
-                            const float2 wk = (g == 0) ? t : cmul(wr0, t);
-                            const float2 wkm = (g == 0) ? tm : cmul(wr1, tm);
                             const float ex = 0.5f * (A.x + Bq.x), ey = 0.5f * (A.y - Bq.y);
                             const float dx = 0.5f * (A.x - Bq.x), dy = 0.5f * (A.y + Bq.y);
+                            const float u = wk.x * dy + wk.y * dx, v = wk.y * dy - wk.x * dx;
                             if (k < sp.fcount && k >= sp.klo && k <= sp.khi) {
-                                const float2 X = make_float2(ex + wk.x * dy + wk.y * dx, ey + wk.y * dy - wk.x * dx);
+                                const float2 X = make_float2(ex + u, ey + v);
                                 const float e = Kc * (X.x * X.x + X.y * X.y);
                                 if (MODE == MODE_SINGLE) sink.put(k, e);
                                 else acc[w * nb + q] += e;
                             }
                             if (km < sp.fcount && km >= sp.klo && km <= sp.khi) {
-                                const float2 Xm = make_float2(ex + wkm.x * dy - wkm.y * dx, -ey + wkm.y * dy + wkm.x * dx);
+                                const float2 Xm = make_float2(ex - u, v - ey);
                                 const float e = Kc * (Xm.x * Xm.x + Xm.y * Xm.y);
                                 if (MODE == MODE_SINGLE) sink.put(km, e);
                                 else acc[w * nb + (pair ? 2 * L - 1 - q : (g == 0 ? L - q : L - 1 - q))] += e;
                             }
-                            t = tn;
+                            wk = cmul(wk, make_float2(kW2L[LOGL].x, kW2L[LOGL].y));
                         }
                         if (g == 0 && tau == TPW - 1) {
-                            // q = L/2, its own mirror; t = W_2L^{L/2}
+                            // q = L/2, its own mirror; wk = W_2L^{L/2}
                             const int k = M * (L / 2);
                             if (k < sp.fcount && k >= sp.klo && k <= sp.khi) {
                                 const float2 A = buf[pad16(o0 + L / 2)];
-                                const float2 X = make_float2(A.x + t.x * A.y, t.y * A.y);
+                                const float2 X = make_float2(A.x + wk.x * A.y, wk.y * A.y);
                                 const float e = Kc * (X.x * X.x + X.y * X.y);
                                 if (MODE == MODE_SINGLE) sink.put(k, e);
                                 else acc[w * nb + L / 2] += e;
@@ -678,50 +683,6 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     }
                     if (!COLLECT && MODE == MODE_SINGLE) sink_reduce<TPW>(sink.best, s_key, w, valid, tid);
                 }
-            } else
-            for (int base = 0; base < ntasks; base += T) {
-                const int task = base + tid;
-                const bool valid = task < ntasks;
-                const int w = valid ? task / TPW : 0;
-                const int tau = task - w * TPW;
-                const int q0 = tau * CH;
-                BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
-                if (valid) {
-                    const bool phase = tau < tlo || tau >= thi;
-                    const int o0 = (w * nf) << LOGL;
-                    const int o1 = o0 + L;
-#pragma unroll 1
-                    for (int h = 0; h < nf; ++h) {
-                        const int rho = h ? rho1 : rho0;
-                        const float2 wr = h ? wr1 : wr0;
-                        const int oa = h ? o1 : o0;                // A = Y_h[q]
-                        const int ob = pair ? (h ? o0 : o1) : o0;  // B = partner FFT
-                        const int pa = pad16(oa + q0);
-                        // partner L - 1 - q for g >= 1: a descending run inside one
-                        // 16-block, since (L - 1 - q0) mod 16 is 15 or 7
-                        const int pb = pad16(ob + L - 1 - q0);
-                        // W_2L^q: the table entry at q0, then one rotation by W_2L per bin
-                        float2 t = __ldg(tw + (q0 << (12 - LOGL)));
-#pragma unroll 2
-                        for (int qq = 0; qq < CH; ++qq) {
-                            const int q = q0 + qq;
-                            const int k = M * q + rho;
-                            const float2 A = buf[pa + qq];
-                            const float2 Bq = (g == 0) ? buf[pad16(ob + ((L - q) & (L - 1)))] : buf[pb - qq];
-                            const float2 wk = (g == 0) ? t : cmul(wr, t);
-                            t = cmul(t, make_float2(kW2L[LOGL].x, kW2L[LOGL].y));
-                            const float ex = 0.5f * (A.x + Bq.x), ey = 0.5f * (A.y - Bq.y);
-                            const float dx = 0.5f * (A.x - Bq.x), dy = 0.5f * (A.y + Bq.y);
-                            const float2 X = make_float2(ex + wk.x * dy + wk.y * dx, ey + wk.y * dy - wk.x * dx);
-                            if (k < sp.fcount && !(phase && (k < sp.klo || k > sp.khi))) {
-                                const float e = Kc * (X.x * X.x + X.y * X.y);
-                                if (MODE == MODE_SINGLE) sink.put(k, e);
-                                else acc[w * nb + q + h * L] += e;
-                            }
-                        }
-                    }
-                }
-                if (!COLLECT && MODE == MODE_SINGLE) sink_reduce<TPW>(sink.best, s_key, w, valid, tid);
             }
             if constexpr (LOGL >= 10 && (MODE == MODE_SINGLE || MODE == MODE_MMP3)) {
                 // (3b) for L >= 1024: the phase-dependent bins one per thread (a
@@ -811,15 +772,15 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     float2 rot = centre_rot((unsigned)(M * q0 + rho), m.z, cf, nfu, tw);
                     const int pa = pad16(oa + q0);
                     const int pb = pad16(ob + L - 1 - q0);
-                    float2 t = __ldg(tw + (q0 << (12 - LOGL)));
+                    // W_Nfft^k = W_Nfft^rho W_2L^q, rotated by W_2L from bin to bin
+                    float2 wk = __ldg(tw + (q0 << (12 - LOGL)));
+                    if (g != 0) wk = cmul(wr, wk);
 #pragma unroll 2
-                    for (int qq = 0; qq < CH; ++qq) {
+                    for (int qq = 0; qq < CH; ++qq, wk = cmul(wk, make_float2(kW2L[LOGL].x, kW2L[LOGL].y))) {
                         const int q = q0 + qq;
                         const int k = M * q + rho;
                         const float2 A = buf[pa + qq];
                         const float2 Bq = (g == 0) ? buf[pad16(ob + ((L - q) & (L - 1)))] : buf[pb - qq];
-                        const float2 wk = (g == 0) ? t : cmul(wr, t);
-                        t = cmul(t, make_float2(kW2L[LOGL].x, kW2L[LOGL].y));
                         if (k < sp.fcount && (k < sp.klo || k > sp.khi)) {
                             const float ex = 0.5f * (A.x + Bq.x), ey = 0.5f * (A.y - Bq.y);
                             const float dx = 0.5f * (A.x - Bq.x), dy = 0.5f * (A.y + Bq.y);
