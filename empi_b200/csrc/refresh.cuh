@@ -266,18 +266,20 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
         constexpr int R0 = 1 << FIRST;
         constexpr int LQ = LOGL - FIRST;  // log2 of L / R0
         // fused first pass: a job's points are jq + rr L / R0
+        // A pair's second FFT input is z conj(W_Nh^{r n}) W_L^n = z conj(t2) with
+        // t2 = W_Nh^{r n} conj(W_L^n), rotated like t.
         const float2 jstep = (FIRST != 0 && g >= 1) ? twist(1 << LQ) : one;
-        const float2 jpstep = (FIRST != 0 && pair) ? pfac(1 << LQ) : one;
+        const float2 j2step = (FIRST != 0 && pair) ? cmulc(jstep, pfac(1 << LQ)) : one;
         // other sizes: a thread's points are np0 + i T within a window
         const int np0 = tid & (L - 1);
         const float2 t0 = (FIRST == 0 && g >= 1) ? twist(np0) : one;
-        const float2 p0 = (FIRST == 0 && pair) ? pfac(np0) : one;
+        const float2 t20 = (FIRST == 0 && pair) ? cmulc(t0, pfac(np0)) : one;
         const float2 tstep = (FIRST == 0 && g >= 1 && L > kUnitThreads) ? twist(kUnitThreads) : one;
-        const float2 pstep = (FIRST == 0 && pair && L > kUnitThreads) ? pfac(kUnitThreads) : one;
+        const float2 t2step = (FIRST == 0 && pair && L > kUnitThreads) ? cmulc(tstep, pfac(kUnitThreads)) : one;
         // (1) load: y_r[n'] = sum_m z[n' + mL] W_Nh^{r (n' + mL)}; for the second
-        // FFT of a pair the sum is conjugate-twisted (and then multiplied by
-        // W_L^{n'} by the caller).  t = the twist at n = np.
-        auto load_point = [&](const int4& m, float cf, int np, float2 t, float2& a1, float2& a2) {
+        // FFT of a pair the sum is conjugate-twisted and multiplied by W_L^{n'}.
+        // t, t2 = the twists at n = np.
+        auto load_point = [&](const int4& m, float cf, int np, float2 t, float2 t2, float2& a1, float2& a2) {
             const float* __restrict__ xs = x + m.x;
             a1 = make_float2(0.f, 0.f);
             a2 = make_float2(0.f, 0.f);
@@ -295,11 +297,12 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                         a1 = z;
                     } else {
                         a1 = cmul(z, t);
-                        if (g >= 2) a2 = cmulc(z, t);
+                        if (g >= 2) a2 = cmulc(z, t2);
                     }
                 }
                 return;
             }
+            const float2 pf = cmulc(t, t2);  // W_L^{np}
             int n = np;
             for (int mm = 0; mm < F; ++mm, n += L) {
                 const int i0 = 2 * n;
@@ -320,6 +323,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     t = cmul(t, fold);
                 }
             }
+            if (g >= 2) a2 = cmul(a2, pf);
         };
         if constexpr (FIRST != 0) {
             // the first Stockham pass (radix 2^FIRST, no twiddles) fused into the load
@@ -329,15 +333,14 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                 const int4 m = s_win[w];
                 const float cf = __int_as_float(m.w);
                 float2 t = g >= 1 ? twist(jq) : one;
-                float2 pf = pair ? pfac(jq) : one;
+                float2 t2 = pair ? cmulc(t, pfac(jq)) : one;
                 float2 v1[R0], v2[R0];
 #pragma unroll
                 for (int rr = 0; rr < R0; ++rr) {
-                    load_point(m, cf, jq + (rr << LQ), t, v1[rr], v2[rr]);
-                    if (pair) v2[rr] = cmul(v2[rr], pf);
+                    load_point(m, cf, jq + (rr << LQ), t, t2, v1[rr], v2[rr]);
                     if (rr + 1 < R0) {
                         t = cmul(t, jstep);
-                        pf = cmul(pf, jpstep);
+                        if (pair) t2 = cmul(t2, j2step);
                     }
                 }
                 // o mod 16 is a multiple of R0, so o + rr keeps o's padding
@@ -362,15 +365,15 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     const float cf = __int_as_float(m.w);
                     // points np0 + i T: padded offsets step by T + T / 16
                     float2* pp = buf + pad16(((w * nf) << LOGL) + np0);
-                    float2 t = t0, pf = p0;
+                    float2 t = t0, t2 = t20;
 #pragma unroll 4
                     for (int np = np0; np < L; np += kUnitThreads, pp += kUnitThreads + kUnitThreads / 16) {
                         float2 a1, a2;
-                        load_point(m, cf, np, t, a1, a2);
+                        load_point(m, cf, np, t, t2, a1, a2);
                         pp[0] = a1;
-                        if (pair) pp[L + L / 16] = cmul(a2, pf);
+                        if (pair) pp[L + L / 16] = a2;
                         t = cmul(t, tstep);
-                        pf = cmul(pf, pstep);
+                        if (pair) t2 = cmul(t2, t2step);
                     }
                 }
             } else {
@@ -379,10 +382,10 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     const int np = idx & (L - 1);
                     const int4 m = s_win[w];
                     float2 a1, a2;
-                    load_point(m, __int_as_float(m.w), np, t0, a1, a2);
+                    load_point(m, __int_as_float(m.w), np, t0, t20, a1, a2);
                     const int o = (w * nf) << LOGL;
                     buf[pad16(o + np)] = a1;
-                    if (pair) buf[pad16(o + L + np)] = cmul(a2, p0);
+                    if (pair) buf[pad16(o + L + np)] = a2;
                 }
             }
             __syncthreads();
