@@ -246,52 +246,95 @@ __global__ void k_sched_a(BatchDev b, int mode, int only_scale, double tA_in, do
     int* units = b.ij_units + ip.ij_off + inst;
     int* chunks = b.ij_chunks + ip.ij_off + inst;
     double st_flops = 0.0, st_bytes = 0.0, st_slots = 0.0;  // statistics, one atomic each per CTA
-    for (int j = threadIdx.x; j < dp.nscales; j += blockDim.x) {
-        const ScalePlan sp = b.scales[dp.scale0 + j];
-        int lo = 0, hi = -1;
-        if (s_active) {
-            if (init) {
-                if (only_scale < 0 || only_scale == j) {
-                    lo = 0;
-                    hi = sp.tcount - 1;
+    // per-scale unit and chunk counts, scanned across the CTA a blockDim-sized
+    // batch of scales at a time into units[j + 1], chunks[j + 1] (inclusive
+    // prefix sums; units[0] = chunks[0] = 0)
+    __shared__ int s_wu[32], s_wc[32], s_carry[2];
+    if (threadIdx.x == 0) {
+        s_carry[0] = 0;
+        s_carry[1] = 0;
+        units[0] = 0;
+        chunks[0] = 0;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int base = 0; base < dp.nscales; base += blockDim.x) {
+        const int j = base + threadIdx.x;
+        int nu = 0, nc = 0;
+        if (j < dp.nscales) {
+            const ScalePlan sp = b.scales[dp.scale0 + j];
+            int lo = 0, hi = -1;
+            if (s_active) {
+                if (init) {
+                    if (only_scale < 0 || only_scale == j) {
+                        lo = 0;
+                        hi = sp.tcount - 1;
+                    }
+                } else {
+                    dirty_range(sp, dp.tMax, s_tA, s_sA, lo, hi);
                 }
-            } else {
-                dirty_range(sp, dp.tMax, s_tA, s_sA, lo, hi);
+            }
+            b.dirty[ip.ij_off + j] = make_int2(lo, hi);
+            int c0 = 0;
+            if (hi >= lo) {
+                const int n = hi - lo + 1;
+                for (int g = 0; g < sp.G; ++g) nu += group_units(n, g, sp);
+                // this scale's units go to the list of its sub-FFT size
+                int at = atomicAdd(b.lcount + sp.logL, nu);
+                const int cap = b.lcap[sp.logL];
+                int4* list = b.units + b.loff[sp.logL];
+                for (int g = 0; g < sp.G; ++g) {
+                    const int B = g >= 2 ? sp.B2 : sp.B1;
+                    for (int t0 = lo; t0 <= hi; t0 += B, ++at)
+                        if (at < cap) list[at] = make_int4(inst, j | (g << 16), t0, min(B, hi - t0 + 1));
+                }
+                const long long s0 = sp.slot_base + (long long)lo * sp.G;
+                const long long s1 = sp.slot_base + (long long)(hi + 1) * sp.G - 1;
+                c0 = (int)(s0 / kChunk);
+                nc = (int)(s1 / kChunk) - c0 + 1;
+                // statistics: reference-equivalent FFT flops (2.5 Nfft log2 Nfft per
+                // window and channel) and compulsory bytes (the FP32 residual span
+                // read once per channel, one 8-byte slot write per (window, group))
+                int iL0, iR0, iL1, iR1;
+                double tf;
+                window_bounds(grid_t(lo, dp.tMax, sp.tcount), sp.hw, dp.fs, dp.N, iL0, iR0, tf);
+                window_bounds(grid_t(hi, dp.tMax, sp.tcount), sp.hw, dp.fs, dp.N, iL1, iR1, tf);
+                const double lg = log2((double)sp.nfft);
+                st_flops += (double)n * ip.C * 2.5 * sp.nfft * lg;
+                st_bytes += 4.0 * ip.C * (double)(iR1 - iL0 + 1) + 8.0 * (double)n * sp.G;
+                st_slots += (double)n * sp.G;
+            }
+            b.ij_crange[ip.ij_off + j] = make_int2(c0, nc);
+        }
+        int iu = nu, ic = nc;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int yu = __shfl_up_sync(0xffffffffu, iu, off), yc = __shfl_up_sync(0xffffffffu, ic, off);
+            if (lane >= off) {
+                iu += yu;
+                ic += yc;
             }
         }
-        b.dirty[ip.ij_off + j] = make_int2(lo, hi);
-        int nu = 0, nc = 0, c0 = 0;
-        if (hi >= lo) {
-            const int n = hi - lo + 1;
-            for (int g = 0; g < sp.G; ++g) nu += group_units(n, g, sp);
-            // this scale's units go to the list of its sub-FFT size
-            int at = atomicAdd(b.lcount + sp.logL, nu);
-            const int cap = b.lcap[sp.logL];
-            int4* list = b.units + b.loff[sp.logL];
-            for (int g = 0; g < sp.G; ++g) {
-                const int B = g >= 2 ? sp.B2 : sp.B1;
-                for (int t0 = lo; t0 <= hi; t0 += B, ++at)
-                    if (at < cap) list[at] = make_int4(inst, j | (g << 16), t0, min(B, hi - t0 + 1));
-            }
-            const long long s0 = sp.slot_base + (long long)lo * sp.G;
-            const long long s1 = sp.slot_base + (long long)(hi + 1) * sp.G - 1;
-            c0 = (int)(s0 / kChunk);
-            nc = (int)(s1 / kChunk) - c0 + 1;
-            // statistics: reference-equivalent FFT flops (2.5 Nfft log2 Nfft per
-            // window and channel) and compulsory bytes (the FP32 residual span
-            // read once per channel, one 8-byte slot write per (window, group))
-            int iL0, iR0, iL1, iR1;
-            double tf;
-            window_bounds(grid_t(lo, dp.tMax, sp.tcount), sp.hw, dp.fs, dp.N, iL0, iR0, tf);
-            window_bounds(grid_t(hi, dp.tMax, sp.tcount), sp.hw, dp.fs, dp.N, iL1, iR1, tf);
-            const double lg = log2((double)sp.nfft);
-            st_flops += (double)n * ip.C * 2.5 * sp.nfft * lg;
-            st_bytes += 4.0 * ip.C * (double)(iR1 - iL0 + 1) + 8.0 * (double)n * sp.G;
-            st_slots += (double)n * sp.G;
+        if (lane == 31) {
+            s_wu[warp] = iu;
+            s_wc[warp] = ic;
         }
-        units[j + 1] = nu;
-        chunks[j + 1] = nc;
-        b.ij_crange[ip.ij_off + j] = make_int2(c0, nc);
+        __syncthreads();
+        int pu = s_carry[0], pc = s_carry[1];
+        for (int wp = 0; wp < warp; ++wp) {
+            pu += s_wu[wp];
+            pc += s_wc[wp];
+        }
+        if (j < dp.nscales) {
+            units[j + 1] = pu + iu;
+            chunks[j + 1] = pc + ic;
+        }
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) {
+            s_carry[0] = pu + iu;
+            s_carry[1] = pc + ic;
+        }
+        __syncthreads();
     }
     {
         __shared__ double s_st[3][32];
@@ -311,15 +354,6 @@ __global__ void k_sched_a(BatchDev b, int mode, int only_scale, double tA_in, do
             double v = 0.0;
             for (int wp = 0; wp < (int)(blockDim.x >> 5); ++wp) v += s_st[threadIdx.x][wp];
             if (v != 0.0) atomicAdd(b.stats + threadIdx.x, v);
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        units[0] = 0;
-        chunks[0] = 0;
-        for (int j = 0; j < dp.nscales; ++j) {
-            units[j + 1] += units[j];
-            chunks[j + 1] += chunks[j];
         }
     }
 }
