@@ -648,7 +648,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                         // D = (A - conj B) / 2i: X[k] = E + W D, X[Nh-k] = conj(E - W D).
                         float2 wk = __ldg(tw + (q0 << (12 - LOGL)));  // W_2L^q
                         if (g != 0) wk = cmul(wr0, wk);
-#pragma unroll 4
+#pragma unroll 8
                         for (int qq = 0; qq < nq; ++qq) {
                             const int q = q0 + qq;
                             const int k = M * q + rho0;
