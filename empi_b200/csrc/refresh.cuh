@@ -399,8 +399,8 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
         // phase-dependent bins, and MMP1 folds the phase into its channel sums:
         // those keep the single pass.
         constexpr bool kSplit = MODE != MODE_MMP1 && LOGL >= 6;
-        if constexpr (!kSplit && (LOGL == 12 || (LOGL >= 3 && LOGL <= 5)) && MODE == MODE_SINGLE) {
-            // (L = 4096 and 8 <= L <= 32.)  Mirrored pairs: bins k and Nh - k read the same two values
+        if constexpr (!kSplit && LOGL >= 3 && MODE == MODE_SINGLE) {
+            // (8 <= L <= 32.)  Mirrored pairs: bins k and Nh - k read the same two values
             // (Z[k], Z[Nh - k]) with A and B exchanged, so one pair of loads
             // gives both.  A task takes q0 .. q0 + nq - 1 and their mirrors: the
             // partner residue's L - 1 - q (pairs, g = 1) or L - q (g = 0, where
@@ -625,7 +625,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
             // window, and only their phase-dependent bins are left to (3b).
             static_assert(MODE == MODE_SINGLE || MODE == MODE_MMP3, "the split spectrum serves SMP and MMP3");
             {
-                // bins k and Nh - k from one pair of loads, as at L = 4096 (the
+                // bins k and Nh - k from one pair of loads, as for 8 <= L <= 32 (the
                 // phase-dependent ones, whichever task holds them, are (3b)'s);
                 // MMP3 adds each channel's energy to the bin's sum instead
                 constexpr int QH = CH / 2;
