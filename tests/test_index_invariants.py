@@ -145,3 +145,22 @@ def test_load_twiddle_indices(logl):
     # W_L^n (pair factor) and W_2L^n (residue M/2) from the 8192-entry table
     assert int(((n & (L - 1)) << (13 - logl)).max()) < TW_N
     assert int(((n & (2 * L - 1)) << (12 - logl)).max()) < TW_N
+
+
+@pytest.mark.parametrize("logl", range(1, 13))
+def test_mmp_channel_sum_indices(logl):
+    # MMP per-bin channel sums: acc[w nb + q'] with nb = L + 1 (group 0, the
+    # Nyquist bin at q' = L), 2L (pairs) or L (residue M/2), held in
+    # kUnitPoints + NW floats per sum
+    L = 1 << logl
+    nw = min(UNIT_POINTS >> logl, MAX_WINDOWS)
+    for g, pair in ((0, False), (1, False), (2, True)):
+        nwin, _ = unit_points(logl, pair)
+        nb = L + 1 if g == 0 else (2 * L if pair else L)
+        q = np.arange(L)
+        direct = q
+        mirrored_q = np.arange(max(L // 2, 1)) if not pair else q
+        mirror = (2 * L - 1 - mirrored_q) if pair else ((L - mirrored_q) if g == 0 else (L - 1 - mirrored_q))
+        idx = np.concatenate([direct, mirror, [L] if g == 0 else [], q + L if pair else []]).astype(int)
+        assert idx.min() >= 0 and idx.max() < nb
+        assert nwin * nb <= UNIT_POINTS + nw
