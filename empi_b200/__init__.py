@@ -75,6 +75,7 @@ EXPORTS = [
     "empi_subtract_atom_from_signal", "empi_batch_create", "empi_batch_destroy", "empi_batch_load",
     "empi_batch_run", "empi_batch_atoms", "empi_batch_total_energy", "empi_batch_get_stats",
     "empi_decompose", "empi_run_config", "empi_book_write", "empi_subtract_atom_from_signal_noalloc",
+    "empi_dictionary_error_bounds",
 ]
 
 _lib = None
@@ -102,6 +103,8 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
                                        ctypes.POINTER(ctypes.c_uint64), ip]
     L.empi_dictionary_scales.argtypes = [ctypes.POINTER(Dictionary), ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                          dp, ip, ip, ip, ip]
+    L.empi_dictionary_error_bounds.argtypes = [ctypes.POINTER(Dictionary), ctypes.c_double, ctypes.c_int,
+                                               ctypes.c_int, fp, fp, fp, ip, ip, ip]
     L.empi_workspace_create.argtypes = [vp, ctypes.POINTER(Dictionary), ctypes.c_double, ctypes.c_int,
                                         ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
     L.empi_workspace_destroy.argtypes = [vp]
@@ -259,6 +262,23 @@ def dictionary_scales(energyError, freqSampling, sampleCount, scaleMin=0.0, scal
     _check(L.empi_dictionary_scales(ctypes.byref(d), freqSampling, int(sampleCount), cap, _dp(s), _ip(nf),
                                     _ip(fc), _ip(tc), ctypes.byref(n)))
     return [(float(s[i]), int(nf[i]), int(fc[i]), int(tc[i])) for i in range(n.value)]
+
+
+def dictionary_error_bounds(energyError, freqSampling, sampleCount, scaleMin=0.0, scaleMax=math.inf,
+                            freqMax=math.inf):
+    """Per scale: (bnd_d, rho, tph, klo, khi) of the engine's certified FP32
+    error bound (include/empi_b200.h, empi_dictionary_error_bounds)."""
+    L = load_library()
+    d = _dictionary(energyError, scaleMin, scaleMax, freqMax)
+    cap = 4096
+    bd, rho, tph = (np.zeros(cap, np.float32) for _ in range(3))
+    klo, khi = np.zeros(cap, np.int32), np.zeros(cap, np.int32)
+    n = ctypes.c_int()
+    fp = ctypes.POINTER(ctypes.c_float)
+    _check(L.empi_dictionary_error_bounds(ctypes.byref(d), freqSampling, int(sampleCount), cap,
+                                          bd.ctypes.data_as(fp), rho.ctypes.data_as(fp), tph.ctypes.data_as(fp),
+                                          _ip(klo), _ip(khi), ctypes.byref(n)))
+    return [(float(bd[i]), float(rho[i]), float(tph[i]), int(klo[i]), int(khi[i])) for i in range(n.value)]
 
 
 # ---------------------------------------------------------------- workspace seam

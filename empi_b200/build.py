@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libempi_b200.so")
+CHECK_LIB = os.path.join(HERE, "libempi_b200_check.so")
 CLI = os.path.join(HERE, "empi-gpu")
 BUILD = os.path.join(HERE, "_build")
 
@@ -51,27 +52,36 @@ def _stale(target, deps) -> bool:
     return not os.path.exists(target) or os.path.getmtime(target) < _newest(deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
+def build(force: bool = False, verbose: bool = False, checked: bool = False) -> str:
+    """Builds the library (and the CLI).  checked=True builds the diagnostic
+    variant libempi_b200_check.so instead: every data-dependent index is
+    bounds-checked on the device (-DEMPI_CHECK); select it with
+    EMPI_B200_LIB."""
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [
         os.path.join(ROOT, "include", "empi_b200.h"), __file__]
-    os.makedirs(BUILD, exist_ok=True)
+    lib = CHECK_LIB if checked else LIB
+    bdir = BUILD + ("_check" if checked else "")
+    extra = ["-DEMPI_CHECK"] if checked else []
+    os.makedirs(bdir, exist_ok=True)
     cc = nvcc()
     ccbin = ["-ccbin", host_cxx()]
-    if force or _stale(LIB, deps):
+    if force or _stale(lib, deps):
         objs = []
         for src in SOURCES:
-            obj = os.path.join(BUILD, src + ".o")
-            cmd = [cc] + ccbin + NVCC_FLAGS + ENGINE_FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
+            obj = os.path.join(bdir, src + ".o")
+            cmd = [cc] + ccbin + NVCC_FLAGS + ENGINE_FLAGS + extra + ["-c", os.path.join(CSRC, src), "-o", obj]
             if src.endswith(".cpp"):
-                cmd = [cc] + ccbin + ["-x", "cu"] + NVCC_FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
+                cmd = [cc] + ccbin + ["-x", "cu"] + NVCC_FLAGS + extra + ["-c", os.path.join(CSRC, src), "-o", obj]
             if verbose:
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)
             objs.append(obj)
-        tmp = LIB + ".tmp"
+        tmp = lib + ".tmp"
         cmd = [cc] + ccbin + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs
         subprocess.run(cmd, check=True)
-        os.replace(tmp, LIB)
+        os.replace(tmp, lib)
+    if checked:
+        return lib
     cli_src = os.path.join(CSRC, "empi_cli.cpp")
     if force or _stale(CLI, [cli_src, LIB]):
         cmd = [host_cxx(), "-O2", "-std=c++17", "-o", CLI, cli_src, "-L" + HERE, "-lempi_b200",
@@ -81,5 +91,4 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
-    print(LIB)
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv, checked="--checked" in sys.argv))

@@ -90,7 +90,7 @@ extern "C" void empi_engine_opts_default(empi_engine_opts* o) {
     if (!o) return;
     std::memset(o, 0, sizeof(*o));
     o->transform_cap = 4096;
-    o->candidate_band = 1e-4;
+    o->candidate_band = 0.0;
     o->candidate_capacity = 0;
     o->iterations_per_graph = 8;
 }
@@ -112,7 +112,7 @@ extern "C" empi_status empi_engine_create(const empi_engine_opts* opts, empi_eng
     if (opts) {
         e->opts = *opts;
         if (e->opts.transform_cap == 0) e->opts.transform_cap = 4096;
-        if (e->opts.candidate_band <= 0) e->opts.candidate_band = 1e-4;
+        if (!(e->opts.candidate_band >= 0.0) || e->opts.candidate_band >= 1.0) e->opts.candidate_band = 0.0;
         if (e->opts.iterations_per_graph <= 0) e->opts.iterations_per_graph = 8;
     }
     int n = 0;
@@ -203,6 +203,28 @@ extern "C" empi_status empi_dictionary_scales(const empi_dictionary* d, double f
     return ok();
 }
 
+extern "C" empi_status empi_dictionary_error_bounds(const empi_dictionary* d, double fs, int samples, int cap,
+                                                    float* bnd_d, float* rho, float* tph, int* klo, int* khi,
+                                                    int* count) {
+    if (!d) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    DictPlan dp;
+    std::vector<ScalePlan> sp;
+    std::vector<float> et;
+    std::string err;
+    if (!build_dictionary(fs, samples, d->energy_error, d->scale_min, d->scale_max, d->freq_max, 4096, dp, sp, et,
+                          nullptr, nullptr, err))
+        return fail(EMPI_ERR_INVALID_ARGUMENT, err);
+    for (int i = 0; i < dp.nscales && i < cap; ++i) {
+        if (bnd_d) bnd_d[i] = sp[i].bnd_d;
+        if (rho) rho[i] = sp[i].bnd_rho;
+        if (tph) tph[i] = sp[i].bnd_tph;
+        if (klo) klo[i] = sp[i].klo;
+        if (khi) khi[i] = sp[i].khi;
+    }
+    if (count) *count = dp.nscales;
+    return ok();
+}
+
 // ------------------------------------------------------------ batch state
 
 namespace {
@@ -217,6 +239,12 @@ struct DevBuf {
     cudaError_t alloc(size_t count) {
         n = std::max<size_t>(count, 1);
         return cudaMalloc(&p, sizeof(T) * n);
+    }
+    // drops the contents: for scratch that is rebuilt every iteration
+    cudaError_t realloc_discard(size_t count) {
+        if (p) cudaFree(p);
+        p = nullptr;
+        return alloc(count);
     }
 };
 
@@ -246,7 +274,10 @@ struct empi_batch {
     DevBuf<DictPlan> d_dicts;
     DevBuf<InstPlan> d_insts;
     DevBuf<int2> d_blk_ic, d_fit_map;
-    DevBuf<float> d_input, d_residual32, d_etab, d_whf;
+    DevBuf<float> d_input, d_input_spare, d_residual32, d_etab, d_whf, d_chan_xmax;
+    cudaStream_t copy_stream = nullptr;  // staged loads of the next batch (batch_stage)
+    cudaEvent_t staged_ev = nullptr;
+    bool staged = false;
     DevBuf<WinGeom> d_wgeom;
     DevBuf<double> d_residual, d_atoms, d_energies, d_chan_energy, d_fit_atoms, d_stats;
     DevBuf<InstState> d_state;
@@ -277,9 +308,12 @@ struct empi_batch {
 
     empi_batch_stats stats{};
     int launches_per_iter = 10;
+    int regrows = 0;  // candidate-buffer growths (overflow recoveries) so far
 
     ~empi_batch() {
         if (graph) cudaGraphExecDestroy(graph);
+        if (copy_stream) cudaStreamSynchronize(copy_stream), cudaStreamDestroy(copy_stream);
+        if (staged_ev) cudaEventDestroy(staged_ev);
         for (auto e : ev) cudaEventDestroy(e);
         if (run_start) cudaEventDestroy(run_start);
         if (run_stop) cudaEventDestroy(run_stop);
@@ -441,8 +475,6 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
     for (int e = 0; e < count; ++e) {
         const empi_epoch& ep = epochs[e];
         if (ep.channels <= 0 || ep.samples <= 0) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidEpochShape");
-        if (ep.channels > kMaxChannels && (variant == EMPI_MMP1 || variant == EMPI_MMP3))
-            return fail(EMPI_ERR_INVALID_ARGUMENT, "tooManyChannels");
         auto key = std::make_pair(ep.fs, ep.samples);
         if (!dict_of.count(key)) {
             DictPlan dp;
@@ -548,6 +580,7 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
     CUDA_TRY(b->d_atoms.alloc(out_off));
     CUDA_TRY(b->d_energies.alloc((size_t)ninst * iters));
     CUDA_TRY(b->d_chan_energy.alloc(cen_off));
+    CUDA_TRY(b->d_chan_xmax.alloc(cen_off));
     CUDA_TRY(b->d_fit_atoms.alloc(b->fit_map.size() * (size_t)iters * 6));
     CUDA_TRY(b->d_stats.alloc(4));
     CUDA_TRY(b->d_state.alloc(ninst));
@@ -635,6 +668,7 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
     d.energies = b->d_energies.p;
     d.indices = b->d_indices.p;
     d.chan_energy = b->d_chan_energy.p;
+    d.chan_xmax = b->d_chan_xmax.p;
     d.stats = b->d_stats.p;
     d.dump = nullptr;
     st = configure(b.get());
@@ -655,10 +689,13 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
 }
 
 empi_status check_errors(empi_batch* b) {
+    int chk = 0;
+    CUDA_TRY(cudaMemcpyAsync(&chk, b->d_ctr.p + CTR_CHECK, sizeof(int), cudaMemcpyDeviceToHost, b->eng->stream));
     std::vector<InstState> st(b->insts.size());
     CUDA_TRY(cudaMemcpyAsync(st.data(), b->d_state.p, sizeof(InstState) * st.size(), cudaMemcpyDeviceToHost,
                              b->eng->stream));
     CUDA_TRY(cudaStreamSynchronize(b->eng->stream));
+    if (chk) return fail(EMPI_ERR_INTERNAL, "boundsCheck:" + std::to_string(chk));  // EMPI_CHECK builds only
     for (size_t i = 0; i < st.size(); ++i) {
         if (st[i].status == ST_ERROR || st[i].err != ERR_NONE) {
             switch (st[i].err) {
@@ -669,6 +706,37 @@ empi_status check_errors(empi_batch* b) {
             }
         }
     }
+    return EMPI_OK;
+}
+
+// Grows the candidate buffers fourfold after an overflow stalled some
+// instances (their contents are per-iteration scratch); the graph, which
+// holds the old pointers, is captured again on the next run step.
+empi_status grow_candidates(empi_batch* b) {
+    BatchDev& d = b->dev;
+    const long long cap = 4LL * std::max(d.cslot_cap, d.cbin_cap);
+    const long long icap = 4LL * d.inst_bin_cap;
+    // at most 2^24 candidate slots / bins (~0.8 GB with their FP64 values at
+    // one channel) and 2^28 per-instance bin ids
+    if (cap > (1LL << 24) || cap * b->cmax > (1LL << 26) || icap * (long long)b->insts.size() > (1LL << 28))
+        return fail(EMPI_ERR_CANDIDATE_OVERFLOW, "candidateOverflow");
+    CUDA_TRY(cudaStreamSynchronize(b->eng->stream));
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    CUDA_TRY(b->d_cslots.realloc_discard((size_t)cap));
+    CUDA_TRY(b->d_cbins.realloc_discard((size_t)cap));
+    CUDA_TRY(b->d_cbin_v.realloc_discard((size_t)cap * b->cmax));
+    CUDA_TRY(b->d_inst_bins.realloc_discard((size_t)icap * b->insts.size()));
+    d.cslots = b->d_cslots.p;
+    d.cbins = b->d_cbins.p;
+    d.cbin_v = b->d_cbin_v.p;
+    d.inst_bins = b->d_inst_bins.p;
+    d.cslot_cap = (int)cap;
+    d.cbin_cap = (int)cap;
+    d.inst_bin_cap = (int)icap;
+    b->regrows++;
     return EMPI_OK;
 }
 
@@ -721,6 +789,7 @@ extern "C" empi_status empi_batch_load(empi_batch* b, const empi_epoch* epochs) 
                                  cudaMemcpyHostToDevice, b->eng->stream));
     }
     CUDA_TRY(cudaStreamSynchronize(b->eng->stream));
+    b->staged = false;  // these epochs replace any staged ones
     return ok();
 }
 
@@ -736,13 +805,64 @@ empi_status batch_load_device(empi_batch* b, const float* const* device_data) {
 
 }  // namespace empi
 
-extern "C" empi_status empi_batch_run(empi_batch* b) {
+extern "C" empi_status empi_batch_run(empi_batch* b) { return batch_run_hooked(b, nullptr); }
+
+namespace empi {
+
+empi_status batch_stage(empi_batch* b, const empi_epoch* epochs) {
+    if (!b || !epochs) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    empi_status st = set_device(b->eng);
+    if (st != EMPI_OK) return st;
+    if (!b->copy_stream) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&b->copy_stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&b->staged_ev, cudaEventDisableTiming));
+    }
+    if (!b->d_input_spare.p) CUDA_TRY(b->d_input_spare.alloc(b->d_input.n));
+    for (size_t e = 0; e < b->epochs.size(); ++e) {
+        if (epochs[e].channels != b->epochs[e].channels || epochs[e].samples != b->epochs[e].samples || !epochs[e].data)
+            return fail(EMPI_ERR_INVALID_ARGUMENT, "epochShapeMismatch");
+        CUDA_TRY(cudaMemcpyAsync(b->d_input_spare.p + b->epoch_in_off[e], epochs[e].data,
+                                 sizeof(float) * (size_t)epochs[e].channels * epochs[e].samples,
+                                 cudaMemcpyHostToDevice, b->copy_stream));
+    }
+    CUDA_TRY(cudaEventRecord(b->staged_ev, b->copy_stream));
+    b->staged = true;
+    return ok();
+}
+
+empi_status batch_loop_progress(empi_batch* b, int epoch, int loop, int* it, int* running, double* etotal,
+                                double* energies) {
+    if (!b || epoch < 0 || epoch >= (int)b->epochs.size()) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    const int i0 = b->epoch_first_inst[epoch];
+    const int loops = b->insts[i0].chan0 >= 0 ? b->epochs[epoch].channels : 1;
+    if (loop < 0 || loop >= loops) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    const int inst = i0 + loop;
+    InstState is;
+    CUDA_TRY(cudaMemcpy(&is, b->d_state.p + inst, sizeof(is), cudaMemcpyDeviceToHost));
+    *it = is.it;
+    *running = is.status == ST_RUNNING || is.status == ST_STALLED;
+    *etotal = is.etotal;
+    if (energies && is.it > 0)
+        CUDA_TRY(cudaMemcpy(energies, b->d_energies.p + (size_t)inst * b->settings.iteration_max,
+                            sizeof(double) * is.it, cudaMemcpyDeviceToHost));
+    return EMPI_OK;
+}
+
+empi_status batch_run_hooked(empi_batch* b, const std::function<void()>& after_chunk) {
     if (!b) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
     empi_status st = set_device(b->eng);
     if (st != EMPI_OK) return st;
     st = capture_graph(b);
     if (st != EMPI_OK) return st;
     cudaStream_t s = b->eng->stream;
+    if (b->staged) {
+        // decompose the epochs staged by batch_stage: wait for their copy and
+        // make their buffer the input (k_init and the MMP2 fit read it)
+        CUDA_TRY(cudaStreamWaitEvent(s, b->staged_ev, 0));
+        std::swap(b->d_input.p, b->d_input_spare.p);
+        b->dev.input = b->d_input.p;
+        b->staged = false;
+    }
     const bool timing = b->eng->opts.timing != 0;
     CUDA_TRY(cudaMemsetAsync(b->d_ctr.p, 0, sizeof(int) * CTR_COUNT, s));
     CUDA_TRY(cudaMemsetAsync(b->d_stats.p, 0, sizeof(double) * 4, s));
@@ -760,20 +880,24 @@ extern "C" empi_status empi_batch_run(empi_batch* b) {
         refresh_ms += ms;
         refresh_launches++;
     }
-    int iters = 0;
     const int imax = b->settings.iteration_max;
-    int active = 1;
     const int K = b->eng->opts.iterations_per_graph;
-    while (iters < imax && active > 0) {
+    // every instance stops itself after imax atoms; a chunk in which some
+    // instances stall on a candidate overflow costs at most one extra chunk
+    const int max_regrows = 12;
+    const int max_chunks = (imax + K - 1) / K + max_regrows + 2;
+    int chunks = 0;
+    for (;;) {
         if (timing) {
             for (int k = 0; k < K; ++k) launch_iteration(b, s, b->ev[2 * (k + 1)], b->ev[2 * (k + 1) + 1]);
             CUDA_TRY(cudaGetLastError());
         } else {
             CUDA_TRY(cudaGraphLaunch(b->graph, s));
         }
-        iters += K;
+        ++chunks;
         launches += K * b->launches_per_iter;
-        CUDA_TRY(cudaMemcpyAsync(&active, b->d_ctr.p + CTR_ACTIVE, sizeof(int), cudaMemcpyDeviceToHost, s));
+        int ctr_now[CTR_COUNT];
+        CUDA_TRY(cudaMemcpyAsync(ctr_now, b->d_ctr.p, sizeof(ctr_now), cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaStreamSynchronize(s));
         if (timing) {
             for (int k = 0; k < K; ++k) {
@@ -783,6 +907,22 @@ extern "C" empi_status empi_batch_run(empi_batch* b) {
                 refresh_launches++;
             }
         }
+        if (after_chunk) after_chunk();
+        if (ctr_now[CTR_STALLED] > 0) {
+            // more candidates than the buffers hold: grow them, resume the
+            // stalled instances (nothing of theirs moved in the stalled step)
+            if (b->regrows >= max_regrows) return fail(EMPI_ERR_CANDIDATE_OVERFLOW, "candidateOverflow");
+            st = grow_candidates(b);
+            if (st != EMPI_OK) return st;
+            st = capture_graph(b);
+            if (st != EMPI_OK) return st;
+            k_unstall<<<std::max(1, std::min(1024, ((int)b->insts.size() + 255) / 256)), 256, 0, s>>>(b->dev);
+            CUDA_TRY(cudaGetLastError());
+            ++launches;
+        } else if (ctr_now[CTR_ACTIVE] == 0) {
+            break;
+        }
+        if (chunks >= max_chunks) return fail(EMPI_ERR_INTERNAL, "iterationLimitExceeded");
     }
     if (!b->fit_map.empty()) {
         k_mmp2_fit<<<(int)b->fit_map.size(), 256, b->max_n * sizeof(double), s>>>(b->dev, b->d_fit_map.p,
@@ -821,6 +961,8 @@ extern "C" empi_status empi_batch_run(empi_batch* b) {
     if (es != EMPI_OK) return es;
     return ok();
 }
+
+}  // namespace empi
 
 extern "C" empi_status empi_batch_atoms(empi_batch* b, int epoch, int cap, double* atoms, int* count,
                                         double* energies, int* indices) {
@@ -953,6 +1095,7 @@ empi_status ws_reset_state(empi_workspace* w) {
     cudaStream_t s = b->eng->stream;
     CUDA_TRY(cudaMemset2DAsync(b->d_state.p, sizeof(InstState), 0, 4 * sizeof(int), b->insts.size(), s));
     CUDA_TRY(cudaMemsetAsync(b->d_ctr.p + CTR_CSLOTS, 0, sizeof(int) * 4, s));
+    CUDA_TRY(cudaMemsetAsync(b->d_ctr.p + CTR_STALLED, 0, sizeof(int), s));
     return EMPI_OK;
 }
 
@@ -999,10 +1142,20 @@ extern "C" empi_status empi_workspace_find_best(empi_workspace* w, double* param
     empi_status st = set_device(b->eng);
     if (st != EMPI_OK) return st;
     cudaStream_t s = b->eng->stream;
-    st = ws_reset_state(w);
-    if (st != EMPI_OK) return st;
-    launch_select(b, s);
-    CUDA_TRY(cudaGetLastError());
+    for (;;) {
+        st = ws_reset_state(w);
+        if (st != EMPI_OK) return st;
+        launch_select(b, s);
+        CUDA_TRY(cudaGetLastError());
+        InstState is;
+        CUDA_TRY(cudaMemcpyAsync(&is, b->d_state.p, sizeof(is), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        if (is.status != ST_STALLED) break;
+        // more candidates than the buffers hold: grow them and select again
+        if (b->regrows >= 12) return fail(EMPI_ERR_CANDIDATE_OVERFLOW, "candidateOverflow");
+        st = grow_candidates(b);
+        if (st != EMPI_OK) return st;
+    }
     st = check_errors(b);
     if (st != EMPI_OK) return st;
     CUDA_TRY(cudaMemcpy(params, b->d_atoms.p, sizeof(double) * 6 * w->C, cudaMemcpyDeviceToHost));
@@ -1090,22 +1243,24 @@ extern "C" empi_status empi_subtract_atom_from_signal(empi_engine* eng, double* 
 
 // Device copy of the signal (EMPI_NOALLOC_MAX_SAMPLES doubles) followed by the
 // six atom params, for empi_subtract_atom_from_signal_noalloc.  It is a fixed
-// static array so callers that may not allocate (stream capture, a device
-// owned by another memory pool) can still run the subtraction; every device
-// that loads the library holds these 8 MiB until exit.
+// static array so callers that may not allocate (a device whose memory another
+// framework's pool owns, a fixed device-memory budget) can still run the
+// subtraction; every device that loads the library holds these 8 MiB until
+// exit.
 static __device__ __align__(256) double g_subtract_staging[EMPI_NOALLOC_MAX_SAMPLES + 8];
 
 namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_staging_mutex;
-double* g_staging_ptr[kMaxDevices] = {};  // device address of the array, per device
+// device address of the array, per device, looked up on the first call with
+// that device current (a later cudaDeviceReset of the device is unsupported)
+double* g_staging_ptr[kMaxDevices] = {};
 }  // namespace
 
 extern "C" empi_status empi_subtract_atom_from_signal_noalloc(int device, void* stream, double* params,
                                                               double* samples, int n, double fs, int fit) {
-    if (!params || !samples || !(fs > 0)) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
-    if (n <= 0 || n > EMPI_NOALLOC_MAX_SAMPLES)
-        return fail(EMPI_ERR_INVALID_ARGUMENT, "signalLongerThanStaticScratch");
+    if (!params || !samples || !(fs > 0) || n <= 0) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    if (n > EMPI_NOALLOC_MAX_SAMPLES) return fail(EMPI_ERR_INVALID_ARGUMENT, "signalLongerThanStaticScratch");
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return fail(EMPI_ERR_NO_DEVICE, "noCudaDevice");
     if (device < 0 || device >= count || device >= kMaxDevices) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidDevice");

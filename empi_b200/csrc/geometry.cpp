@@ -24,6 +24,63 @@ int ilog2(long x) {
     return l;
 }
 
+// Worst-case FP32 error of the refresh's window values, as constants per
+// scale (unit roundoff u = 2^-24; every count below rounds up).
+//
+// Each computed value X32_k is a linear function of the window's packed
+// samples z_n = x_{2n} g_{2n} + i x_{2n+1} g_{2n+1}.  Along the computation
+// (fold, twist, Stockham passes, unpacking) every intermediate value is a
+// unit-modulus-weighted sum of a subset of the z_n, so its modulus is at most
+// A = sum_n |x_n| g_n, and a rounding error made at one stage reaches X_k
+// through unit-modulus factors.  Summing the worst relative error of each
+// stage therefore gives |X32_k - X_k| <= eta A with, in units of u:
+//   residual rounded to FP32                          1
+//   Gaussian exp2f (approximate) and its argument     6
+//   sample product                                    2
+//   twist W_Nh^{rn}: table product plus up to 8
+//     rotations, and its complex product              40
+//   each fold: sum plus fold rotation                 4 per fold (F)
+//   each Stockham pass: W^k rotated up to 15 times
+//     and the in-register radix-16 DFT                64 per pass (P)
+// counted twice (X_k = E + W D combines Z[k] and Z[Nh - k]), plus the
+// unpacking and the W_2L rotation of up to 8 bins   40.
+// A <= max|x| (sum_n g_n + W 2^-20), and sum_n g_n <= s fs + 1 for a
+// Gaussian of width s fs >= 2 samples (Poisson summation); the 2^-20 per
+// sample covers the exp2f absolute error where g is tiny.
+//
+// The energy is a norm of X: for a single channel fs |v|^2 normReal^2 =
+// Kc |X|^2 / (1 + e cos 2phi'), the maximum over phases of a quadratic form
+// whose eigenvalues lie in [Kc / (1 + e), Kc / (1 - e)] (e = expFactor), so
+// sqrt(E) moves by at most sqrt(Kc / (1 - e)) |X32 - X| (summed over channels
+// by Minkowski's inequality for MMP3, and for MMP1's constrained sums).
+// Phase-dependent bins (k != 0, Nh; bins 0 and Nh are real) have
+// e <= e1 = exp(-2 pi (s fs / Nfft)^2), bnd_rho = 1 / (1 - e1).  Their
+// closed-form energy Kc p^2 / (p + e Re(X^2 e^{i psi})) divides by
+// D >= p (1 - e): rounding in D (8 u) and the magnitude error of the
+// rotated e^{i psi} (60 u) are amplified by bnd_rho, its angle error (180 u)
+// by at most e / sqrt(1 - e^2) <= sqrt(bnd_rho); the rest adds 7 u.
+void set_error_bound(ScalePlan& p, double fs) {
+    const double u = std::ldexp(1.0, -24);
+    const int first = p.logL & 3;
+    const int passes = (first ? 1 : 0) + (p.logL - first) / 4;
+    const double eta = u * (2.0 * (1 + 6 + 2 + 40 + 4.0 * p.F + 64.0 * passes) + 40);
+    const double width = p.s * fs + 1.0 + p.wmax * std::ldexp(1.0, -20);
+    p.bnd_d = (float)(eta * width * (1.0 + 1e-6));
+    const long Nh = p.nfft / 2;
+    // any phase-dependent bin other than k = 0 and k = Nh
+    const bool low = p.klo > 1, high = p.khi < p.fcount - 1 && std::min<long>(p.fcount - 1, Nh - 1) > p.khi;
+    double rho = 1.0;
+    if (low || high) {
+        const double x = p.s * fs / p.nfft;
+        const double e1 = std::exp(-2.0 * M_PI * x * x);
+        rho = 1.0 / (1.0 - e1);
+    }
+    p.bnd_rho = (float)(rho * (1.0 + 1e-6));
+    p.bnd_srho = (float)(std::sqrt(rho) * (1.0 + 1e-6));
+    p.bnd_tph = (float)(u * (7.0 + rho * (8.0 + 60.0) + 2.0 * std::sqrt(rho) * 180.0));
+    p.sKc = (float)(std::sqrt(2.0 * M_SQRT2 / (p.s * fs)) * (1.0 + 1e-6));
+}
+
 }  // namespace
 
 bool build_dictionary(double fs, int N, double energyError, double scaleMin, double scaleMax,
@@ -177,6 +234,7 @@ bool build_dictionary(double fs, int N, double energyError, double scaleMin, dou
         p.Kc = (float)(2.0 * M_SQRT2 / (s * fs));
         p.K1 = (float)(M_SQRT2 / (s * fs));
         p.aG2 = (float)(std::sqrt(M_PI) / (s * fs) * std::sqrt(1.0 / std::log(2.0)));
+        set_error_bound(p, fs);
         slots += (long long)tCount * p.G;
         values += (unsigned long long)fCount * (unsigned long long)tCount;
         scales.push_back(p);

@@ -38,10 +38,23 @@ enum Counter {
     CTR_STAT_UNITS = 9,  // running totals for statistics
     CTR_STAT_SLOTS = 10,
     CTR_STAT_BINS = 11,
+    CTR_STALLED = 12,    // instances stalled by a candidate overflow since the last regrowth
+    CTR_CHECK = 13,      // (EMPI_CHECK builds) largest code of a failed bounds check
     CTR_COUNT = 16
 };
 
-enum Status { ST_RUNNING = 0, ST_DONE = 1, ST_ERROR = 2 };
+// Bounds self-checks of the data-dependent indices, compiled in with
+// -DEMPI_CHECK (a diagnostic build, not the product): a failed check records
+// its code in ctr[CTR_CHECK] and the access is skipped instead of made.
+#ifdef EMPI_CHECK
+#define EMPI_BAD(cond, code) ((cond) ? (atomicMax(b.ctr + CTR_CHECK, (code)), true) : false)
+#else
+#define EMPI_BAD(cond, code) false
+#endif
+
+// ST_STALLED: the candidate buffers overflowed in this iteration; the
+// instance took no step and resumes once the host has grown the buffers
+enum Status { ST_RUNNING = 0, ST_DONE = 1, ST_ERROR = 2, ST_STALLED = 3 };
 enum ErrCode { ERR_NONE = 0, ERR_SIGNAL_EMPTY = 4, ERR_MAP_EMPTY = 5, ERR_CAND_OVERFLOW = 7 };
 
 struct InstPlan {
@@ -54,7 +67,9 @@ struct InstPlan {
 struct InstState {
     int status, it, err, nbins;
     double etotal, eres;
-    unsigned long long best32;
+    unsigned long long best32;  // tree root: upper-bound bits << 32 | slot
+    float bnorm;                // channel norm of max |residual| (the error bound's B)
+    unsigned tstar;             // certified lower bound of the best exact energy (float bits)
 };
 
 struct CandSlot {
@@ -107,6 +122,7 @@ struct BatchDev {
     double* energies;   // ninst x iter_max
     int4* indices;      // ninst x iter_max: (scale, t, f, -)
     double* chan_energy;  // per (instance, channel)
+    float* chan_xmax;     // per (instance, channel): max |FP32 residual|
     double* stats;        // [0] reference-equivalent FFT flops, [1] algorithmic bytes, [2] slots
     float* dump;          // optional energy-map dump [f][t] of one scale
 };
@@ -192,6 +208,19 @@ __device__ __forceinline__ float2 twiddle_pow2(unsigned m, unsigned n, const flo
     return make_float2(c, s);
 }
 
+// max over a CTA of non-negative floats (ordered as their bit patterns);
+// valid in every thread; red holds 32 words
+__device__ __forceinline__ float block_max_nonneg(float v, unsigned* red) {
+    unsigned x = __reduce_max_sync(0xffffffffu, __float_as_uint(fmaxf(v, 0.0f)));
+    if (threadIdx.x < 32) red[threadIdx.x] = 0u;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) atomicMax(red, x);
+    __syncthreads();
+    x = red[0];
+    __syncthreads();
+    return __uint_as_float(x);
+}
+
 #include "refresh.cuh"
 
 // ------------------------------------------------------------ schedule
@@ -234,6 +263,8 @@ __global__ void k_sched_a(BatchDev b, int mode, int only_scale, double tA_in, do
             if (e / st.etotal <= b.residual_energy) {
                 st.status = ST_DONE;
                 active = 0;
+            } else if (EMPI_BAD(st.it < 1, 13)) {
+                active = 0;
             } else {
                 const double* p = b.atoms + ip.out_off + (long long)(st.it - 1) * ip.C * 6;
                 s_tA = p[2] / dp.fs;
@@ -243,6 +274,27 @@ __global__ void k_sched_a(BatchDev b, int mode, int only_scale, double tA_in, do
         s_active = active;
     }
     __syncthreads();
+    if (mode == SCHED_ATOM) {
+        // the caller changed a channel's residual (the workspace seam): its
+        // largest |sample| anew
+        __shared__ unsigned redm[32];
+        for (int c = 0; c < ip.C; ++c) {
+            const float* x32 = b.residual32 + ip.res_off + (long long)c * dp.N;
+            float xm = 0.0f;
+            for (int i = threadIdx.x; i < dp.N; i += blockDim.x) xm = fmaxf(xm, fabsf(x32[i]));
+            xm = block_max_nonneg(xm, redm);
+            if (threadIdx.x == 0) b.chan_xmax[ip.cen_off + c] = xm;
+        }
+    }
+    if (threadIdx.x == 0) {
+        // B of the refresh's error bound: the channel norm of max |residual|
+        double q = 0.0;
+        for (int c = 0; c < ip.C; ++c) {
+            const double xm = (double)b.chan_xmax[ip.cen_off + c];
+            q += xm * xm;
+        }
+        b.state[inst].bnorm = __double2float_ru(sqrt(q));
+    }
     int* units = b.ij_units + ip.ij_off + inst;
     int* chunks = b.ij_chunks + ip.ij_off + inst;
     double st_flops = 0.0, st_bytes = 0.0, st_slots = 0.0;  // statistics, one atomic each per CTA
@@ -428,6 +480,7 @@ __global__ void k_tree(BatchDev b) {
         const int j = upper_index(b.ij_chunks + ip.ij_off + inst, dp.nscales, rem);
         rem -= b.ij_chunks[ip.ij_off + inst + j];
         const int chunk = b.ij_crange[ip.ij_off + j].x + rem;
+        if (EMPI_BAD(chunk < 0 || chunk >= dp.chunks, 12)) continue;
         const long long s0 = (long long)chunk * kChunk;
         const long long s1 = min(s0 + kChunk, dp.slots);
         const unsigned long long* sl = b.slots + ip.slot_off;
@@ -483,13 +536,16 @@ __device__ __forceinline__ void slot_to_jtg(const BatchDev& b, const DictPlan& d
     g = (int)(rel - (long long)t * sp.G);
 }
 
-// One CTA per instance: the root of the tournament tree (the instance's best
-// over its chunk maxima), then every slot whose FP32 max is within the band of
-// it becomes a candidate (qualifying chunks first, then their slots).
+// One CTA per instance: the root of the tournament tree (the slot with the
+// largest certified upper bound U), whose certified lower bound L is a lower
+// bound of the best exact energy; every slot whose U reaches it is a candidate
+// (a warp per qualifying leaf chunk), and the largest L among the candidates
+// becomes the instance's threshold tstar for the bins (k_collect).  No slot
+// outside the candidates can hold the exact maximum, whatever the FP32 error.
 __global__ void k_cand_slots(BatchDev b) {
-    __shared__ int s_chunks[256];
-    __shared__ int s_n;
     __shared__ unsigned long long red[32];
+    __shared__ unsigned long long s_root;
+    __shared__ unsigned s_tstar;
     const int inst = blockIdx.x;
     InstState& st = b.state[inst];
     if (st.status != ST_RUNNING) return;
@@ -501,42 +557,34 @@ __global__ void k_cand_slots(BatchDev b) {
         root = v > root ? v : root;
     }
     root = block_max_u64(root, red);  // valid in thread 0
-    __shared__ unsigned long long s_root;
     if (threadIdx.x == 0) {
         st.best32 = root;
+        st.nbins = 0;
         s_root = root;
     }
     __syncthreads();
-    const unsigned best = (unsigned)(s_root >> 32);
-    if (best == 0u) {  // nothing beats 0: src/gabor.cpp:108-110
+    if ((unsigned)(s_root >> 32) == 0u) {  // nothing beats 0: src/gabor.cpp:108-110
         if (threadIdx.x == 0) {
             st.status = ST_ERROR;
             st.err = ERR_MAP_EMPTY;
         }
         return;
     }
-    const unsigned thr = __float_as_uint(__uint_as_float(best) * (1.0f - b.band));
-    if (threadIdx.x == 0) {
-        st.nbins = 0;
-        s_n = 0;
-    }
+    const long long rs = (long long)(s_root & 0xffffffffull);
+    if (EMPI_BAD(rs >= dp.slots, 1)) return;
+    const float lroot = __uint_as_float((unsigned)(b.slots[ip.slot_off + rs] & 0xffffffffull));
+    const unsigned tbits = __float_as_uint(lroot * (1.0f - b.band));
+    if (threadIdx.x == 0) s_tstar = __float_as_uint(lroot);
     __syncthreads();
-    for (int c = threadIdx.x; c < dp.chunks; c += blockDim.x) {
-        if ((unsigned)(b.chunks[ip.chunk_off + c] >> 32) >= thr) {
-            const int at = atomicAdd(&s_n, 1);
-            if (at < 256) s_chunks[at] = c;
-            else st.err = ERR_CAND_OVERFLOW;
-        }
-    }
-    __syncthreads();
-    const int nc = min(s_n, 256);
-    for (int ic = 0; ic < nc; ++ic) {
-        const int c = s_chunks[ic];
+    const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    for (int c = threadIdx.x >> 5; c < dp.chunks; c += nwarps) {
+        if ((unsigned)(b.chunks[ip.chunk_off + c] >> 32) < tbits) continue;
         const long long s0 = (long long)c * kChunk;
         const long long s1 = min(s0 + kChunk, dp.slots);
-        for (long long s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+        for (long long s = s0 + lane; s < s1; s += 32) {
             const unsigned long long v = b.slots[ip.slot_off + s];
-            if ((unsigned)(v >> 32) >= thr) {
+            if ((unsigned)(v >> 32) >= tbits) {
+                atomicMax(&s_tstar, (unsigned)(v & 0xffffffffull));
                 const int at = atomicAdd(b.ctr + CTR_CSLOTS, 1);
                 if (at < b.cslot_cap) {
                     CandSlot cs;
@@ -549,6 +597,8 @@ __global__ void k_cand_slots(BatchDev b) {
             }
         }
     }
+    __syncthreads();
+    if (threadIdx.x == 0) st.tstar = __float_as_uint(__uint_as_float(s_tstar) * (1.0f - b.band));
 }
 
 // FP64 value of one candidate bin and channel by direct DFT over its window
@@ -565,7 +615,9 @@ __global__ void k_rescore(BatchDev b) {
         __syncthreads();
         if (item >= total) break;
         const int bin = item / b.cmax, c = item - bin * b.cmax;
+        if (EMPI_BAD(bin >= b.cbin_cap, 5)) continue;
         const CandBin cb = b.cbins[bin];
+        if (EMPI_BAD(cb.inst < 0 || cb.inst >= b.ninst, 5)) continue;
         const InstPlan ip = b.insts[cb.inst];
         if (c >= ip.C) continue;
         const DictPlan dp = b.dicts[ip.dict];
@@ -576,6 +628,8 @@ __global__ void k_rescore(BatchDev b) {
         double t0fixed;
         window_bounds(t0, sp.hw, fs, dp.N, iL, iR, t0fixed);
         const int W = iR - iL + 1;
+        if (EMPI_BAD(iL < 0 || iR >= dp.N || cb.j < 0 || cb.j >= dp.nscales || cb.t < 0 || cb.t >= sp.tcount, 5))
+            continue;
         // gaussize, src/gabor.cpp:31-40
         const double wg = sqrt(CUDART_PI) / sp.s;
         const double ga = wg * (1.0 / fs);
@@ -645,19 +699,22 @@ __device__ __forceinline__ Computer64 make_computer64(const ScalePlan& sp, const
     return q;
 }
 
-__device__ __forceinline__ void mmp1_constraint64(double2* v, int C) {
+// Mmp1Decomposition::constraint (src/mmp.cpp:9-21) in two passes over the
+// channel values of one bin (stride 1 in global memory), so any channel count
+// works: the common angle from sum v_c^2, then each channel's projection.
+__device__ __forceinline__ double mmp1_angle64(const double2* v, int C) {
     double dr = 0.0, di = 0.0;
     for (int c = 0; c < C; ++c) {
-        dr += v[c].x * v[c].x - v[c].y * v[c].y;
-        di += 2.0 * v[c].x * v[c].y;
+        const double2 w = v[c];
+        dr += w.x * w.x - w.y * w.y;
+        di += 2.0 * w.x * w.y;
     }
-    const double angle = 0.5 * atan2(di, dr);
-    double sa, ca;
-    sincos(angle, &sa, &ca);
-    for (int c = 0; c < C; ++c) {
-        const double rho = hypot(v[c].x, v[c].y) * cos(atan2(v[c].y, v[c].x) - angle);
-        v[c] = make_double2(rho * ca, rho * sa);
-    }
+    return 0.5 * atan2(di, dr);
+}
+
+__device__ __forceinline__ double2 mmp1_project64(double2 w, double angle, double sa, double ca) {
+    const double rho = hypot(w.x, w.y) * cos(atan2(w.y, w.x) - angle);
+    return make_double2(rho * ca, rho * sa);
 }
 
 __device__ __forceinline__ double norm_real(const Computer64& q, double phase) {
@@ -665,15 +722,13 @@ __device__ __forceinline__ double norm_real(const Computer64& q, double phase) {
     return 1.41421356237309504880 * q.normComplex / sqrt(1.0 + cos(2 * p4) * q.expFactor);
 }
 
-constexpr int kMaxChannels = 64;
-
 // One CTA per instance: FP64 energies of its candidate bins, argmax (ties to
 // the lowest (scale, t, f)), atom parameters (src/gabor.cpp:111-131).
 __global__ void k_select(BatchDev b) {
     __shared__ double s_e[128];
     __shared__ unsigned long long s_key[128];
     __shared__ int s_bin[128];
-    __shared__ double2 s_v[kMaxChannels];
+    __shared__ double s_angle;
     const int inst = blockIdx.x;
     InstState& st = b.state[inst];
     if (st.status != ST_RUNNING) return;
@@ -681,29 +736,44 @@ __global__ void k_select(BatchDev b) {
     const DictPlan dp = b.dicts[ip.dict];
     const int C = ip.C;
     const int nbins = min(st.nbins, b.inst_bin_cap);
-    if (st.err == ERR_CAND_OVERFLOW || nbins == 0) {
+    if (st.err == ERR_CAND_OVERFLOW) {
+        // some candidate did not fit: take no step; the host grows the
+        // buffers and resumes the instance (k_unstall)
+        if (threadIdx.x == 0) {
+            st.status = ST_STALLED;
+            atomicAdd(b.ctr + CTR_STALLED, 1);
+        }
+        return;
+    }
+    if (nbins == 0) {
         if (threadIdx.x == 0) {
             st.status = ST_ERROR;
-            if (st.err == ERR_NONE) st.err = ERR_MAP_EMPTY;
+            st.err = ERR_MAP_EMPTY;
         }
         return;
     }
     double be = -1.0;
     unsigned long long bk = ~0ull;
     int bbin = -1;
-    double2 v[kMaxChannels];
     for (int i = threadIdx.x; i < nbins; i += blockDim.x) {
         const int bin = b.inst_bins[(long long)inst * b.inst_bin_cap + i];
+        if (EMPI_BAD(bin < 0 || bin >= b.cbin_cap, 6)) continue;
         const CandBin cb = b.cbins[bin];
         const ScalePlan sp = b.scales[dp.scale0 + cb.j];
         const Computer64 q = make_computer64(sp, dp, cb.k, cb.t);
-        for (int c = 0; c < C; ++c) v[c] = b.cbin_v[(long long)bin * b.cmax + c];
-        if (b.mode == MODE_MMP1 && !q.isHighFreq) mmp1_constraint64(v, C);
+        const double2* v = b.cbin_v + (long long)bin * b.cmax;
+        const bool constrain = b.mode == MODE_MMP1 && !q.isHighFreq;
+        double angle = 0.0, sa = 0.0, ca = 1.0;
+        if (constrain) {
+            angle = mmp1_angle64(v, C);
+            sincos(angle, &sa, &ca);
+        }
         double square = 0.0;
         for (int c = 0; c < C; ++c) {
-            const double phase = atan2(v[c].y, v[c].x);
+            const double2 w = constrain ? mmp1_project64(v[c], angle, sa, ca) : v[c];
+            const double phase = atan2(w.y, w.x);
             const double nr = norm_real(q, phase);
-            const double mod = hypot(v[c].x, v[c].y) * nr * sqrt(dp.fs);
+            const double mod = hypot(w.x, w.y) * nr * sqrt(dp.fs);
             square += mod * mod;
         }
         b.cbins[bin].e64 = square;
@@ -732,17 +802,19 @@ __global__ void k_select(BatchDev b) {
         __syncthreads();
     }
     const int win = s_bin[0];
+    if (EMPI_BAD(win < 0 || win >= b.cbin_cap, 7)) return;
     const CandBin cb = b.cbins[win];
     const ScalePlan sp = b.scales[dp.scale0 + cb.j];
     const Computer64 q = make_computer64(sp, dp, cb.k, cb.t);
-    if (threadIdx.x == 0) {
-        for (int c = 0; c < C; ++c) s_v[c] = b.cbin_v[(long long)win * b.cmax + c];
-        if (b.mode == MODE_MMP1 && !q.isHighFreq) mmp1_constraint64(s_v, C);
-    }
+    const double2* v = b.cbin_v + (long long)win * b.cmax;
+    const bool constrain = b.mode == MODE_MMP1 && !q.isHighFreq;
+    if (threadIdx.x == 0) s_angle = constrain ? mmp1_angle64(v, C) : 0.0;
     __syncthreads();
+    double sa = 0.0, ca = 1.0;
+    if (constrain) sincos(s_angle, &sa, &ca);
     const int it = st.it;
     for (int c = threadIdx.x; c < C; c += blockDim.x) {
-        const double2 vc = s_v[c];
+        const double2 vc = constrain ? mmp1_project64(v[c], s_angle, sa, ca) : v[c];
         const double phase = atan2(vc.y, vc.x);
         const double nr = norm_real(q, phase);
         const double mag = hypot(vc.x, vc.y);
@@ -836,9 +908,18 @@ __global__ void k_subtract(BatchDev b) {
     }
     __syncthreads();
     double s = 0.0;
-    for (int i = threadIdx.x; i < dp.N; i += blockDim.x) s += x[i] * x[i];
+    float xm = 0.0f;
+    for (int i = threadIdx.x; i < dp.N; i += blockDim.x) {
+        s += x[i] * x[i];
+        xm = fmaxf(xm, fabsf(x32[i]));
+    }
     s = block_sum(s, red);
-    if (threadIdx.x == 0) b.chan_energy[ip.cen_off + c] = s / fs;
+    __shared__ unsigned redm[32];
+    xm = block_max_nonneg(xm, redm);
+    if (threadIdx.x == 0) {
+        b.chan_energy[ip.cen_off + c] = s / fs;
+        b.chan_xmax[ip.cen_off + c] = xm;
+    }
 }
 
 // One CTA per (instance, channel): residual from the float32 input
@@ -855,6 +936,7 @@ __global__ void k_init(BatchDev b, int from_input) {
     const int Cin = ip.in_channels;
     double* x = b.residual + ip.res_off + (long long)c * dp.N;
     double s = 0.0;
+    float xm = 0.0f;
     for (int i = threadIdx.x; i < dp.N; i += blockDim.x) {
         double v;
         if (!from_input) {
@@ -870,10 +952,14 @@ __global__ void k_init(BatchDev b, int from_input) {
         if (from_input) x[i] = v;
         b.residual32[ip.res_off + (long long)c * dp.N + i] = (float)v;
         s += v * v;
+        xm = fmaxf(xm, fabsf((float)v));
     }
     s = block_sum(s, red);
+    __shared__ unsigned redm[32];
+    xm = block_max_nonneg(xm, redm);
     if (threadIdx.x == 0) {
         b.chan_energy[ip.cen_off + c] = s / dp.fs;
+        b.chan_xmax[ip.cen_off + c] = xm;
         if (c == 0) {
             InstState& st = b.state[inst];
             st.status = ST_RUNNING;
@@ -881,8 +967,24 @@ __global__ void k_init(BatchDev b, int from_input) {
             st.err = ERR_NONE;
             st.nbins = 0;
             st.best32 = 0;
+            st.bnorm = 0.0f;
+            st.tstar = 0u;
         }
     }
+}
+
+// Resumes the instances a candidate overflow stalled, once the host has
+// grown the candidate buffers.
+__global__ void k_unstall(BatchDev b) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < b.ninst; i += gridDim.x * blockDim.x) {
+        InstState& st = b.state[i];
+        if (st.status == ST_STALLED) {
+            st.status = ST_RUNNING;
+            st.err = ERR_NONE;
+            st.nbins = 0;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) b.ctr[CTR_STALLED] = 0;
 }
 
 // Workspace::subtractAtomFromSignal on one FP64 signal (src/gabor.cpp:143-187),

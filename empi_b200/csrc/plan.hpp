@@ -47,6 +47,15 @@ struct ScalePlan {
     float K1;          // sqrt(2) / (s fs): MMP1 energy factor
     float aG2;         // aG sqrt(log2 e): Gaussian as exp2(-(d aG2)^2)
     int eoff;          // offset of this scale's expFactor table (bins k < klo, then k > khi)
+    // Certified FP32 error bound of the refresh (see refresh.cuh, "error
+    // bound"): |X32_k - X_k| <= bnd_d * B for every bin of a window, B the
+    // instance's channel norm of max |residual|; phase-dependent bins scale
+    // it by sqrt(bnd_rho) and carry the relative formula error bnd_tph.
+    float bnd_d;       // eta (s fs + 1 + wmax 2^-20): FFT error per unit of max |x|
+    float bnd_rho;     // 1 / (1 - expFactor) of the worst phase-dependent bin (1 if none)
+    float bnd_srho;    // sqrt(bnd_rho)
+    float bnd_tph;     // relative error of a phase-dependent bin's energy formula
+    float sKc;         // sqrt(Kc)
     int pad_;
 };
 

@@ -52,16 +52,24 @@ struct RefreshSmem {
     static constexpr size_t buf = 0;
     static constexpr size_t win = buf + sizeof(float2) * kBufFloat2;  // int4 (iL, W, ci, cf bits)
     static constexpr size_t rot = win + sizeof(int4) * NW;            // float4 (hrot, step)
-    static constexpr size_t key = rot + sizeof(float4) * NW;          // u32 energy bits
-    static constexpr size_t etab = key + sizeof(unsigned) * NW;       // float, kEtabSmem
+    static constexpr size_t key = rot + sizeof(float4) * NW;          // u32 max over non-phase bins
+    static constexpr size_t keyp = key + sizeof(unsigned) * NW;       // u32 max over phase-dependent bins
+    static constexpr size_t etab = keyp + sizeof(unsigned) * NW;      // float, kEtabSmem
     static constexpr size_t acc = etab + sizeof(float) * kEtabSmem;   // (MMP) per-bin channel sums
 };
 
+// (MMP1) per-window certified upper / lower bounds of the constrained
+// phase-dependent bins, after the channel sums
 template <int MODE, int LOGL>
-constexpr size_t refresh_smem_bytes() {
+constexpr size_t refresh_bnd_offset() {
     return RefreshSmem<LOGL>::acc + (MODE == MODE_SINGLE ? 0
                                                        : sizeof(float) * (kUnitPoints + RefreshSmem<LOGL>::NW) *
                                                              (MODE == MODE_MMP1 ? 3 : 1));
+}
+
+template <int MODE, int LOGL>
+constexpr size_t refresh_smem_bytes() {
+    return refresh_bnd_offset<MODE, LOGL>() + (MODE == MODE_MMP1 ? 2 * sizeof(unsigned) * RefreshSmem<LOGL>::NW : 0);
 }
 
 // e^{i psi} with psi = 2 theta_kk = 2 pi (2 kk c / Nfft), c = ci + cf the
@@ -100,64 +108,164 @@ __device__ __forceinline__ float energy_mmp1(float P, float2 S, bool phase, floa
 }
 
 __device__ __forceinline__ void emit_candidate(const BatchDev& b, int inst, int j, int t, int k, float e) {
+    if (EMPI_BAD(inst < 0 || inst >= b.ninst || k < 0, 4)) return;
     const int slot = atomicAdd(b.ctr + CTR_CBINS, 1);
-    if (slot < b.cbin_cap) {
-        const int li = atomicAdd(&b.state[inst].nbins, 1);
-        if (li < b.inst_bin_cap) {
-            CandBin cb;
-            cb.inst = inst;
-            cb.j = j;
-            cb.t = t;
-            cb.k = k;
-            cb.e32 = e;
-            cb.pad = 0;
-            cb.e64 = 0.0;
-            b.cbins[slot] = cb;
-            b.inst_bins[(long long)inst * b.inst_bin_cap + li] = slot;
-            return;
-        }
+    if (slot >= b.cbin_cap) {
+        b.state[inst].err = ERR_CAND_OVERFLOW;
+        return;
     }
-    b.state[inst].err = ERR_CAND_OVERFLOW;
+    // every counted record is written, even when the instance's own list is
+    // full: k_rescore re-scores all of them
+    CandBin cb;
+    cb.inst = inst;
+    cb.j = j;
+    cb.t = t;
+    cb.k = k;
+    cb.e32 = e;
+    cb.pad = 0;
+    cb.e64 = 0.0;
+    b.cbins[slot] = cb;
+    const int li = atomicAdd(&b.state[inst].nbins, 1);
+    if (li < b.inst_bin_cap) b.inst_bins[(long long)inst * b.inst_bin_cap + li] = slot;
+    else b.state[inst].err = ERR_CAND_OVERFLOW;
 }
 
-// What the spectrum stage does with a bin's final energy.  The slot keeps only
-// its maximum energy (the tree keys slots by index); negative, NaN and
-// infinite energies count as 0, as in pack_key.
+// ------------------------------------------------------------ error bound
+//
+// For every bin of a window |X32_k - X_k| <= dlt = bnd_d * B (B = channel norm
+// of max |residual|, geometry.cpp's set_error_bound), and sqrt(energy) is a
+// norm of X, so the exact (FP64) energy E of a bin whose FP32 energy is e
+// satisfies
+//   (sqrt(e (1 - tau)) - d)^2 <= E <= (sqrt(e (1 + tau)) + d)^2
+// with d = sqrt(Kc) dlt (times sqrt(bnd_rho) for phase-dependent bins) and tau
+// the relative error of the energy formula.  Both ends grow with e, so a
+// window needs only the largest e of each class (non-phase, phase-dependent).
+// The slot key stores the upper bound U (high word, ranked by the tree) and
+// the lower bound L (low word).  Margins of 8-16 u cover the FP32 evaluation
+// of the bounds themselves.
+constexpr float kU = 5.9604645e-8f;  // 2^-24
+
+struct BoundTerms {
+    float d_np, d_ph, tau_np, tau_ph;
+};
+
+__device__ __forceinline__ BoundTerms bound_terms(const ScalePlan& sp, float bnorm, int C) {
+    BoundTerms t;
+    const float dlt = sp.bnd_d * bnorm * (1.0f + 8.0f * kU);
+    t.d_np = sp.sKc * dlt;
+    t.d_ph = t.d_np * sp.bnd_srho;
+    const float tc = (float)(2 * (C + 4)) * kU;  // channel sums (MMP1 / MMP3)
+    t.tau_np = 8.0f * kU + tc;
+    t.tau_ph = sp.bnd_tph + tc;
+    return t;
+}
+
+// upper and lower bound of the exact energy of a bin class whose largest FP32
+// energy has code `code` (float bits + 1; 0: no bin of this class)
+__device__ __forceinline__ void class_bounds(unsigned code, float d, float tau, float& U, float& L) {
+    if (!code) {
+        U = 0.0f;
+        L = 0.0f;
+        return;
+    }
+    const float e = __uint_as_float(code - 1u);
+    const float su = sqrtf(e * (1.0f + tau)) * (1.0f + 8.0f * kU) + d;
+    U = su * su * (1.0f + 16.0f * kU);
+    const float sl = sqrtf(e * fmaxf(0.0f, 1.0f - tau)) * (1.0f - 8.0f * kU) - d;
+    L = sl > 0.0f ? sl * sl * (1.0f - 16.0f * kU) : 0.0f;
+}
+
+// smallest FP32 energy of a class whose upper bound can reach tstar
+__device__ __forceinline__ unsigned class_threshold(float tstar, float d, float tau) {
+    const float r = sqrtf(tstar) * (1.0f - 8.0f * kU) - d;
+    if (r <= 0.0f) return 0u;
+    return __float_as_uint(r * r / (1.0f + tau) * (1.0f - 16.0f * kU));
+}
+
+// MMP1, constrained phase-dependent bin (k < klo, src/mmp.cpp:9-21 then
+// src/gabor.cpp:54-71): E = Kc Q / (1 + e cos a) with Q = (P + |S|) / 2 the
+// best common-phase projection energy (a squared seminorm of the channel
+// values) and a = arg S + psi.  Q moves like a norm; the angle a moves by at
+// most asin(|dS| / |S|) plus the rotation's angle error, and the factor is
+// bounded over that interval (or by 1 / (1 -+ e) when |dS| >= |S|).
+// At k = 0 the values are real, exactly and in FP32 (X = Re Z + Im Z), so S
+// is real and non-negative, a = 0 and the factor is 1 / (1 + e) with e = 1.
+__device__ __forceinline__ void mmp1_phase_bounds(float P, float2 S, float e, float2 rot, float Kc, float dlt,
+                                                  int C, bool dc, float& U, float& L) {
+    const float tq = (float)(2 * (C + 4)) * kU;
+    const float as = sqrtf(S.x * S.x + S.y * S.y);
+    const float Q = 0.5f * (P + as);
+    const float su = sqrtf(Q * (1.0f + tq)) * (1.0f + 8.0f * kU) + dlt;
+    const float sl = sqrtf(Q * (1.0f - tq)) * (1.0f - 8.0f * kU) - dlt;
+    const float dS = 2.0f * sqrtf(P) * dlt + dlt * dlt + tq * P;
+    float fup = 1.0f / (1.0f - e), flo = 1.0f / (1.0f + e);
+    if (dc) {
+        fup = flo;
+    } else if (dS < as) {
+        const float ca = fminf(1.0f, fmaxf(-1.0f, (S.x * rot.x - S.y * rot.y) / as));
+        const float a = acosf(ca);
+        const float da = asinf(dS / as) * (1.0f + 1e-5f) + 2e-5f;
+        fup = 1.0f / (1.0f + e * cosf(fminf(3.14159265f, a + da)) - 1e-6f);
+        flo = 1.0f / (1.0f + e * cosf(fmaxf(0.0f, a - da)) + 1e-6f);
+        fup = fminf(fup, 1.0f / (1.0f - e));
+        flo = fmaxf(flo, 1.0f / (1.0f + e));
+    }
+    const float rho = dc ? 1.0f : 1.0f / (1.0f - e);
+    U = Kc * su * su * fup * (1.0f + (76.0f * rho + 24.0f) * kU);
+    L = sl > 0.0f ? Kc * sl * sl * flo * (1.0f - (76.0f * rho + 24.0f) * kU) : 0.0f;
+}
+
+// What the spectrum stage does with a bin's final energy.  Refresh: keep the
+// largest energy of each class (non-phase / phase-dependent bins) as float
+// bits + 1 (0: no bin); negative, NaN and infinite energies count as 0.
+// Collect: emit the bins whose upper bound reaches the instance's certified
+// lower bound tstar, i.e. whose energy is at least its class threshold.
 template <bool COLLECT>
 struct BinSink {
     const BatchDev& b;
     int inst, j, t, tcount;
-    unsigned thr_bits;
-    float best;
-    __device__ __forceinline__ void put(int k, float e) {
+    unsigned thr_np, thr_ph;
+    unsigned best_np, best_ph;
+    __device__ __forceinline__ void put(int k, float e, bool ph) {
         if (COLLECT) {
-            if (__float_as_uint(e) >= thr_bits) emit_candidate(b, inst, j, t, k, e);
+            if (__float_as_uint(e) >= (ph ? thr_ph : thr_np) && e <= 3.0e38f) emit_candidate(b, inst, j, t, k, e);
         } else {
             if (b.dump) b.dump[(long long)k * tcount + t] = e;
-            best = fmaxf(best, e <= 3.0e38f ? e : 0.0f);
+            const unsigned v = __float_as_uint(e >= 0.0f && e <= 3.0e38f ? e : 0.0f) + 1u;
+            if (ph) best_ph = max(best_ph, v);
+            else best_np = max(best_np, v);
+        }
+    }
+    // a bin with explicit bounds (MMP1's constrained phase-dependent bins)
+    __device__ __forceinline__ void put_bounded(int k, float e, float U, float L, float tstar, unsigned* s_ub,
+                                                unsigned* s_lb, int w) {
+        if (COLLECT) {
+            if (U >= tstar) emit_candidate(b, inst, j, t, k, e);
+        } else {
+            if (b.dump) b.dump[(long long)k * tcount + t] = e;
+            atomicMax(s_ub + w, __float_as_uint(U));
+            atomicMax(s_lb + w, __float_as_uint(L));
         }
     }
 };
 
-// Max of one window's bins over the lanes holding its tasks (TPW consecutive,
-// aligned lanes) into the window's shared key; non-negative floats order as
-// their bit patterns.
+// Max of one window's class maxima over the lanes holding its tasks (TPW
+// consecutive, aligned lanes) into the window's shared keys.
 template <int TPW>
-__device__ __forceinline__ void sink_reduce(float bestf, unsigned* s_key, int w, bool valid, int tid) {
-    unsigned best = __float_as_uint(bestf);
+__device__ __forceinline__ void sink_reduce(unsigned best, unsigned* s_key, int w, bool valid, int tid) {
     if (TPW >= 32) {
         best = __reduce_max_sync(0xffffffffu, best);
-        if ((tid & 31) == 0 && valid) atomicMax(s_key + w, best);
+        if ((tid & 31) == 0 && valid && best) atomicMax(s_key + w, best);
     } else {
 #pragma unroll
         for (int off = TPW / 2; off; off >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, off));
-        if ((tid & (TPW - 1)) == 0 && valid) atomicMax(s_key + w, best);
+        if ((tid & (TPW - 1)) == 0 && valid && best) atomicMax(s_key + w, best);
     }
 }
 
 template <int LOGL, int MODE, bool COLLECT>
 __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem, int inst, int j, int g, int t_start,
-                                          int nwin, unsigned thr_bits) {
+                                          int nwin, float tstar) {
     constexpr int L = 1 << LOGL;
     constexpr int CH = L < kBinsPerTask ? L : kBinsPerTask;  // q values per task
     constexpr int TPW = L / CH;                                // tasks per window
@@ -166,11 +274,22 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
     float4* s_rot = reinterpret_cast<float4*>(smem + RefreshSmem<LOGL>::rot);
     float* s_etab = reinterpret_cast<float*>(smem + RefreshSmem<LOGL>::etab);
     unsigned* s_key = reinterpret_cast<unsigned*>(smem + RefreshSmem<LOGL>::key);
+    unsigned* s_keyp = reinterpret_cast<unsigned*>(smem + RefreshSmem<LOGL>::keyp);
     float* acc = reinterpret_cast<float*>(smem + RefreshSmem<LOGL>::acc);
+    unsigned* s_ub = reinterpret_cast<unsigned*>(smem + refresh_bnd_offset<MODE, LOGL>());
+    unsigned* s_lb = s_ub + RefreshSmem<LOGL>::NW;
 
+    if (EMPI_BAD(inst < 0 || inst >= b.ninst, 10)) return;
     const InstPlan ip = b.insts[inst];
     const DictPlan dp = b.dicts[ip.dict];
+    if (EMPI_BAD(j < 0 || j >= dp.nscales, 10)) return;
     const ScalePlan sp = b.scales[dp.scale0 + j];
+    if (EMPI_BAD(sp.logL != LOGL || g < 0 || g >= sp.G || t_start < 0 || nwin < 1 ||
+                     t_start + nwin > sp.tcount || nwin > RefreshSmem<LOGL>::NW, 10))
+        return;
+    if (EMPI_BAD(MODE != MODE_SINGLE && nwin * (g == 0 ? (1 << LOGL) + 1 : (g >= 2 ? 2 << LOGL : 1 << LOGL)) >
+                                            kUnitPoints + RefreshSmem<LOGL>::NW, 8))
+        return;
     const int M = sp.M, F = sp.F;
     const int Nh = sp.nfft >> 1;
     const unsigned nfu = (unsigned)sp.nfft;
@@ -182,6 +301,12 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
     const int tid = threadIdx.x, T = blockDim.x;
     const float2* __restrict__ tw = b.tw;
     const float aG2 = sp.aG2, Kc = sp.Kc;
+    // certified error bound of this unit's bins (see "error bound" above)
+    const float bnorm = b.state[inst].bnorm;
+    const BoundTerms bt = bound_terms(sp, bnorm, ip.C);
+    const float dlt = sp.bnd_d * bnorm * (1.0f + 8.0f * kU);
+    const unsigned thr_np = COLLECT ? class_threshold(tstar, bt.d_np, bt.tau_np) : 0u;
+    const unsigned thr_ph = COLLECT ? class_threshold(tstar, bt.d_ph, bt.tau_ph) : 0u;
 
     // Per window: geometry, and for the phase-dependent bins e^{-2 pi i fs t0}
     // (high bins) and the step of psi from q to q + 1; the scale's expFactor
@@ -192,13 +317,19 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
     {
         const long long w0 = sp.win_base + t_start;
         for (int w = tid; w < nwin; w += T) {
-            const int4 m = __ldg(b.wtab + w0 + w);
+            int4 m = __ldg(b.wtab + w0 + w);
+            if (EMPI_BAD(m.x < 0 || m.y < 1 || m.x + m.y > dp.N, 11)) m.y = 0;
             s_win[w] = m;
             float sh, ch;
             sincospif(-2.0f * __ldg(b.whf + w0 + w), &sh, &ch);
             const float2 st = centre_rot((unsigned)sp.M, m.z, __int_as_float(m.w), (unsigned)sp.nfft, b.tw);
             s_rot[w] = make_float4(ch, sh, st.x, st.y);
             s_key[w] = 0u;
+            s_keyp[w] = 0u;
+            if (MODE == MODE_MMP1) {
+                s_ub[w] = 0u;
+                s_lb[w] = 0u;
+            }
         }
         if (etab_smem)
             for (int i = tid; i < ecount; i += T) s_etab[i] = __ldg(b.etab + sp.eoff + i);
@@ -411,7 +542,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                 const bool valid = task < ntasks;
                 const int w = valid ? task / TPW : 0;
                 const int tau = task - w * TPW;
-                BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
+                BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_np, thr_ph, 0u, 0u};
                 if (valid) {
                     const int4 m = s_win[w];
                     const float cf = __int_as_float(m.w);
@@ -457,7 +588,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                             const bool pk = phase && (k < sp.klo || k > sp.khi);
                             const float e = pk ? energy_phase(X, efac(k), k >= sp.khf ? cmul(rot, hrot) : rot, Kc)
                                                : Kc * (X.x * X.x + X.y * X.y);
-                            sink.put(k, e);
+                            sink.put(k, e, pk);
                         }
                         if (km < sp.fcount) {
                             const bool pk = phase && (km < sp.klo || km > sp.khi);
@@ -468,7 +599,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                             } else {
                                 e = Kc * (Xm.x * Xm.x + Xm.y * Xm.y);
                             }
-                            sink.put(km, e);
+                            sink.put(km, e, pk);
                         }
                         if (phase) rot = cmul(rot, step);
                         wk = cmul(wk, make_float2(kW2L[LOGL].x, kW2L[LOGL].y));
@@ -490,11 +621,14 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                             } else {
                                 e = Kc * (X.x * X.x + X.y * X.y);
                             }
-                            sink.put(k, e);
+                            sink.put(k, e, pk);
                         }
                     }
                 }
-                if (!COLLECT) sink_reduce<TPW>(sink.best, s_key, w, valid, tid);
+                if (!COLLECT) {
+                    sink_reduce<TPW>(sink.best_np, s_key, w, valid, tid);
+                    sink_reduce<TPW>(sink.best_ph, s_keyp, w, valid, tid);
+                }
             }
         } else if constexpr (!kSplit) {
             for (int base = 0; base < ntasks; base += T) {
@@ -502,7 +636,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                 const bool valid = task < ntasks;
                 const int w = valid ? task / TPW : 0;
                 const int q0 = (task - w * TPW) * CH;
-                BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
+                BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_np, thr_ph, 0u, 0u};
                 if (valid) {
                     const int4 m = s_win[w];
                     const float cf = __int_as_float(m.w);
@@ -551,7 +685,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                                     if (pk) e = energy_phase(X, efac(k),
                                                              k >= sp.khf ? cmul(rot, hrot) : rot, Kc);
                                     else e = Kc * (X.x * X.x + X.y * X.y);
-                                    if (MODE == MODE_SINGLE) sink.put(k, e);
+                                    if (MODE == MODE_SINGLE) sink.put(k, e, pk);
                                     else acc[ai] += e;
                                 } else {
                                     acc[ai] += X.x * X.x + X.y * X.y;
@@ -571,7 +705,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                         const float e = pk ? energy_phase(X, efac(Nh),
                                                           cmul(centre_rot((unsigned)Nh, m.z, cf, nfu, tw), hrot), Kc)
                                            : Kc * X.x * X.x;
-                        if (MODE == MODE_SINGLE) sink.put(Nh, e);
+                        if (MODE == MODE_SINGLE) sink.put(Nh, e, pk);
                         else acc[w * nb + L] += e;
                     }
                     if (MODE != MODE_SINGLE && last) {
@@ -589,15 +723,21 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                                 const int k = nyq ? Nh : M * q + rho;
                                 if (k < sp.fcount && !(nyq && h == 1)) {
                                     const int ai = w * nb + q + h * L;
-                                    float e;
                                     if (MODE == MODE_MMP3 || k >= sp.khf) {
-                                        e = acc[ai];
+                                        sink.put(k, acc[ai], k < sp.klo || k > sp.khi);
                                     } else {
                                         const bool pk = k < sp.klo;
-                                        e = energy_mmp1(acc[ai], make_float2(acc[nwin * nb + ai], acc[2 * nwin * nb + ai]),
-                                                        pk, pk ? efac(k) : 0.0f, rot, sp.K1);
+                                        const float P = acc[ai];
+                                        const float2 S = make_float2(acc[nwin * nb + ai], acc[2 * nwin * nb + ai]);
+                                        const float e = energy_mmp1(P, S, pk, pk ? efac(k) : 0.0f, rot, sp.K1);
+                                        if (pk) {
+                                            float Ub, Lb;
+                                            mmp1_phase_bounds(P, S, efac(k), rot, Kc, dlt, ip.C, k == 0, Ub, Lb);
+                                            sink.put_bounded(k, e, Ub, Lb, tstar, s_ub, s_lb, w);
+                                        } else {
+                                            sink.put(k, e, false);
+                                        }
                                     }
-                                    sink.put(k, e);
                                 }
                                 if (phase && MODE == MODE_MMP1 && !nyq) rot = cmul(rot, step);
                             }
@@ -605,17 +745,9 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     }
                 }
                 if (!COLLECT && (MODE == MODE_SINGLE || last)) {
-                    // max over the lanes of this window (TPW consecutive, aligned lanes);
-                    // non-negative floats order as their bit patterns
-                    unsigned best = __float_as_uint(sink.best);
-                    if (TPW >= 32) {
-                        best = __reduce_max_sync(0xffffffffu, best);
-                        if ((tid & 31) == 0 && valid) atomicMax(s_key + w, best);
-                    } else {
-    #pragma unroll
-                        for (int off = TPW / 2; off; off >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, off));
-                        if ((tid & (TPW - 1)) == 0 && valid) s_key[w] = best;
-                    }
+                    // class maxima over the lanes of this window
+                    sink_reduce<TPW>(sink.best_np, s_key, w, valid, tid);
+                    sink_reduce<TPW>(sink.best_ph, s_keyp, w, valid, tid);
                 }
             }
         } else {
@@ -634,7 +766,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     const bool valid = task < ntasks;
                     const int w = valid ? task / TPW : 0;
                     const int tau = task - w * TPW;
-                    BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
+                    BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_np, thr_ph, 0u, 0u};
                     if (valid) {
                         const int nq = pair ? CH : QH;
                         const int q0 = tau * nq;
@@ -661,13 +793,13 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                             if (k < sp.fcount && k >= sp.klo && k <= sp.khi) {
                                 const float2 X = make_float2(ex + u, ey + v);
                                 const float e = Kc * (X.x * X.x + X.y * X.y);
-                                if (MODE == MODE_SINGLE) sink.put(k, e);
+                                if (MODE == MODE_SINGLE) sink.put(k, e, false);
                                 else acc[w * nb + q] += e;
                             }
                             if (km < sp.fcount && km >= sp.klo && km <= sp.khi) {
                                 const float2 Xm = make_float2(ex - u, v - ey);
                                 const float e = Kc * (Xm.x * Xm.x + Xm.y * Xm.y);
-                                if (MODE == MODE_SINGLE) sink.put(km, e);
+                                if (MODE == MODE_SINGLE) sink.put(km, e, false);
                                 else acc[w * nb + (pair ? 2 * L - 1 - q : (g == 0 ? L - q : L - 1 - q))] += e;
                             }
                             wk = cmul(wk, make_float2(kW2L[LOGL].x, kW2L[LOGL].y));
@@ -679,12 +811,12 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                                 const float2 A = buf[pad16(o0 + L / 2)];
                                 const float2 X = make_float2(A.x + wk.x * A.y, wk.y * A.y);
                                 const float e = Kc * (X.x * X.x + X.y * X.y);
-                                if (MODE == MODE_SINGLE) sink.put(k, e);
+                                if (MODE == MODE_SINGLE) sink.put(k, e, false);
                                 else acc[w * nb + L / 2] += e;
                             }
                         }
                     }
-                    if (!COLLECT && MODE == MODE_SINGLE) sink_reduce<TPW>(sink.best, s_key, w, valid, tid);
+                    if (!COLLECT && MODE == MODE_SINGLE) sink_reduce<TPW>(sink.best_np, s_key, w, valid, tid);
                 }
             }
             if constexpr (LOGL >= 10 && (MODE == MODE_SINGLE || MODE == MODE_MMP3)) {
@@ -744,9 +876,9 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     const float2 rot = centre_rot((unsigned)k, m.z, cf, nfu, tw);
                     const float e = energy_phase(X, efac(k), k >= sp.khf ? cmul(rot, hrot) : rot, Kc);
                     if constexpr (MODE == MODE_SINGLE) {
-                        BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
-                        sink.put(k, e);
-                        if (!COLLECT) atomicMax(s_key + w, __float_as_uint(sink.best));
+                        BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_np, thr_ph, 0u, 0u};
+                        sink.put(k, e, true);
+                        if (!COLLECT) atomicMax(s_keyp + w, sink.best_ph);
                     } else {
                         acc[w * nb + aq] += e;
                     }
@@ -758,7 +890,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                 const int w = i / nph;
                 const int jx = i - w * nph;
                 const int q0 = (jx < tlo ? jx : thi + (jx - tlo)) * CH;
-                BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
+                BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_np, thr_ph, 0u, 0u};
                 const int4 m = s_win[w];
                 const float cf = __int_as_float(m.w);
                 const float4 hr = s_rot[w];
@@ -789,7 +921,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                             const float dx = 0.5f * (A.x - Bq.x), dy = 0.5f * (A.y + Bq.y);
                             const float2 X = make_float2(ex + wk.x * dy + wk.y * dx, ey + wk.y * dy - wk.x * dx);
                             const float e = energy_phase(X, efac(k), k >= sp.khf ? cmul(rot, hrot) : rot, Kc);
-                            if (MODE == MODE_SINGLE) sink.put(k, e);
+                            if (MODE == MODE_SINGLE) sink.put(k, e, true);
                             else acc[w * nb + q + h * L] += e;
                         }
                         rot = cmul(rot, step);
@@ -803,10 +935,13 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     const float e = pk ? energy_phase(X, efac(Nh),
                                                       cmul(centre_rot((unsigned)Nh, m.z, cf, nfu, tw), hrot), Kc)
                                        : Kc * X.x * X.x;
-                    if (MODE == MODE_SINGLE) sink.put(Nh, e);
+                    if (MODE == MODE_SINGLE) sink.put(Nh, e, pk);
                     else acc[w * nb + L] += e;
                 }
-                if (!COLLECT && MODE == MODE_SINGLE) atomicMax(s_key + w, __float_as_uint(sink.best));
+                if (!COLLECT && MODE == MODE_SINGLE) {
+                    if (sink.best_ph) atomicMax(s_keyp + w, sink.best_ph);
+                    if (sink.best_np) atomicMax(s_key + w, sink.best_np);
+                }
             }
             if (MODE == MODE_MMP3 && last) {
                 // energies of the accumulated channels
@@ -816,7 +951,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                     const bool valid = task < ntasks;
                     const int w = valid ? task / TPW : 0;
                     const int q0 = (task - w * TPW) * CH;
-                    BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_bits, 0.0f};
+                    BinSink<COLLECT> sink{b, inst, j, t_start + w, sp.tcount, thr_np, thr_ph, 0u, 0u};
                     if (valid) {
                         const int nq = (g == 0 && q0 == 0) ? CH + 1 : CH;
 #pragma unroll 1
@@ -827,11 +962,15 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                                 const bool nyq = qq == CH;
                                 const int q = nyq ? L : q0 + qq;
                                 const int k = nyq ? Nh : M * q + rho;
-                                if (k < sp.fcount && !(nyq && h == 1)) sink.put(k, acc[w * nb + q + h * L]);
+                                if (k < sp.fcount && !(nyq && h == 1))
+                                    sink.put(k, acc[w * nb + q + h * L], k < sp.klo || k > sp.khi);
                             }
                         }
                     }
-                    if (!COLLECT) sink_reduce<TPW>(sink.best, s_key, w, valid, tid);
+                    if (!COLLECT) {
+                        sink_reduce<TPW>(sink.best_np, s_key, w, valid, tid);
+                        sink_reduce<TPW>(sink.best_ph, s_keyp, w, valid, tid);
+                    }
                 }
             }
         }
@@ -839,8 +978,22 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
     }
 
     if (!COLLECT) {
+        // slot key: certified upper bound (high word) and lower bound (low word)
+        // of the exact energies of the slot's bins
         unsigned long long* out = b.slots + ip.slot_off + sp.slot_base;
-        for (int w = tid; w < nwin; w += T) out[(long long)(t_start + w) * sp.G + g] = (unsigned long long)s_key[w] << 32;
+        for (int w = tid; w < nwin; w += T) {
+            float Un, Ln, Up, Lp;
+            class_bounds(s_key[w], bt.d_np, bt.tau_np, Un, Ln);
+            class_bounds(s_keyp[w], bt.d_ph, bt.tau_ph, Up, Lp);
+            float U = fmaxf(Un, Up), Lo = fmaxf(Ln, Lp);
+            if (MODE == MODE_MMP1) {
+                U = fmaxf(U, __uint_as_float(s_ub[w]));
+                Lo = fmaxf(Lo, __uint_as_float(s_lb[w]));
+            }
+            if (!(U <= 3.0e38f)) U = 3.0e38f;  // NaN / inf inputs: keep the slot competitive
+            out[(long long)(t_start + w) * sp.G + g] =
+                ((unsigned long long)__float_as_uint(U) << 32) | (unsigned long long)__float_as_uint(Lo);
+        }
     }
     __syncthreads();
 }
@@ -849,8 +1002,8 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
 // boundary of an out-of-line body cost more than the larger kernel).
 template <int LOGL, int MODE>
 __device__ __forceinline__ void collect_body(const BatchDev& b, unsigned char* smem, int inst, int j, int g, int t,
-                                          unsigned thr_bits) {
-    unit_body<LOGL, MODE, true>(b, smem, inst, j, g, t, 1, thr_bits);
+                                             float tstar) {
+    unit_body<LOGL, MODE, true>(b, smem, inst, j, g, t, 1, tstar);
 }
 
 #ifndef EMPI_REFRESH_MIN_BLOCKS
@@ -872,12 +1025,12 @@ __global__ void __launch_bounds__(kUnitThreads, EMPI_REFRESH_MIN_BLOCKS) k_refre
         __syncthreads();
         if (u >= total) break;
         const int4 un = list[u];  // (instance, scale | group << 16, t_start, nwin)
-        unit_body<LOGL, MODE, false>(b, smem, un.x, un.y & 0xffff, un.y >> 16, un.z, un.w, 0u);
+        unit_body<LOGL, MODE, false>(b, smem, un.x, un.y & 0xffff, un.y >> 16, un.z, un.w, 0.0f);
     }
 }
 
 // FP32 recompute of the candidate slots (one window each), emitting every bin
-// within the band of the instance's best.
+// whose certified upper bound reaches the instance's lower bound tstar.
 template <int MODE>
 __global__ void __launch_bounds__(kUnitThreads, 1) k_collect(BatchDev b) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -890,12 +1043,18 @@ __global__ void __launch_bounds__(kUnitThreads, 1) k_collect(BatchDev b) {
         __syncthreads();
         if (u >= total) break;
         const CandSlot cs = b.cslots[u];
-        const unsigned best = (unsigned)(b.state[cs.inst].best32 >> 32);
-        const unsigned thr = __float_as_uint(__uint_as_float(best) * (1.0f - b.band));
+        if (EMPI_BAD(cs.inst < 0 || cs.inst >= b.ninst, 2)) continue;
+        const float tstar = __uint_as_float(b.state[cs.inst].tstar);
         const InstPlan ip = b.insts[cs.inst];
-        switch (b.scales[b.dicts[ip.dict].scale0 + cs.j].logL) {
+        if (EMPI_BAD(cs.j < 0 || cs.j >= b.dicts[ip.dict].nscales, 2)) continue;
+        const ScalePlan& sp = b.scales[b.dicts[ip.dict].scale0 + cs.j];
+        if (EMPI_BAD(cs.t < 0 || cs.t >= sp.tcount || cs.g < 0 || cs.g >= sp.G, 3)) continue;
+        // slots below the refined threshold hold no candidate bin
+        const unsigned long long key = b.slots[ip.slot_off + sp.slot_base + (long long)cs.t * sp.G + cs.g];
+        if (__uint_as_float((unsigned)(key >> 32)) < tstar) continue;
+        switch (sp.logL) {
 #define EMPI_COLLECT_CASE(LG) \
-    case LG: collect_body<LG, MODE>(b, smem, cs.inst, cs.j, cs.g, cs.t, thr); break;
+    case LG: collect_body<LG, MODE>(b, smem, cs.inst, cs.j, cs.g, cs.t, tstar); break;
             EMPI_COLLECT_CASE(0)
             EMPI_COLLECT_CASE(1)
             EMPI_COLLECT_CASE(2)

@@ -41,7 +41,7 @@ typedef enum {
     EMPI_ERR_SIGNAL_IS_EMPTY = 4,      /* signalIsEmpty (src/classes.cpp:35-39) */
     EMPI_ERR_ENERGY_MAP_IS_EMPTY = 5,  /* energyMapIsEmpty (src/gabor.cpp:108-110) */
     EMPI_ERR_SIGNAL_TOO_LONG = 6,      /* signalFileIsTooLongForThisDecomposition */
-    EMPI_ERR_CANDIDATE_OVERFLOW = 7,   /* more near-tied candidates than the engine holds */
+    EMPI_ERR_CANDIDATE_OVERFLOW = 7,   /* candidates beyond the largest buffers the engine grows to */
     EMPI_ERR_CONFIG = 8,               /* configuration errors (src/empi.cpp:59-141) */
     EMPI_ERR_IO = 9,                   /* file errors (src/io.cpp) */
     EMPI_ERR_NO_DEVICE = 10,
@@ -66,8 +66,11 @@ typedef struct {
     int device;              /* CUDA ordinal */
     void* stream;            /* cudaStream_t to run on; NULL = engine-owned stream */
     int transform_cap;       /* largest shared-memory sub-FFT (16..4096, power of 2); 0 = default */
-    double candidate_band;   /* relative FP32 band re-scored in FP64; 0 = default (1e-4) */
-    int candidate_capacity;  /* candidate bins per iteration over a batch; 0 = default */
+    double candidate_band;   /* extra relative margin below the certified lower bound of the best
+                                exact energy when selecting candidates (0 = none, the default:
+                                the certified FP32 error bound alone decides) */
+    int candidate_capacity;  /* initial candidate slots / bins per iteration over a batch
+                                (0 = default); the buffers grow on demand */
     int iterations_per_graph;/* MP iterations per CUDA-graph launch; 0 = default */
     int timing;              /* nonzero: record CUDA events around every refresh launch */
 } empi_engine_opts;
@@ -93,6 +96,19 @@ empi_status empi_dictionary_size(const empi_dictionary* dict, double fs, int sam
  * as the reference's prepareWorkspace builds them.  Arrays hold cap entries. */
 empi_status empi_dictionary_scales(const empi_dictionary* dict, double fs, int samples, int cap,
                                    double* s, int* nfft, int* fcount, int* tcount, int* count);
+
+/* Certified FP32 error bound of the engine's energy maps, per scale (no
+ * counterpart in the reference, whose maps are FP64): for every bin of a
+ * window whose channels' largest |sample| have norm B, the FP32 window value
+ * is within bnd_d * B of the exact one, and
+ *   (sqrt(e32 (1 - tau)) - d)^2 <= exact energy <= (sqrt(e32 (1 + tau)) + d)^2
+ * with d = sqrt(Kc) bnd_d B, Kc = 2 sqrt(2) / (s fs), tau = (8 + 2 (C + 4)) 2^-24
+ * for bins klo <= k <= khi, and d scaled by sqrt(rho), tau = tph + 2 (C + 4) 2^-24
+ * for the phase-dependent bins k < klo or k > khi.  Candidates for the FP64
+ * re-scoring are selected with these bounds, so the argmax is exact. */
+empi_status empi_dictionary_error_bounds(const empi_dictionary* dict, double fs, int samples, int cap,
+                                         float* bnd_d, float* rho, float* tph, int* klo, int* khi,
+                                         int* count);
 
 /* -------------------------------------------------- workspace (the seam) */
 
@@ -132,17 +148,23 @@ empi_status empi_subtract_atom_from_signal(empi_engine* engine, double* params, 
                                            int n, double fs, int fit);
 
 /* Same as empi_subtract_atom_from_signal, for callers that cannot allocate
- * device memory: code running inside CUDA stream capture, or next to a
- * framework whose memory pool owns the device (cudaMalloc and cudaFree are
- * not allowed in the first case and also synchronise the whole device).  No
- * counterpart in the reference: the device copy of the signal and params
- * lives in a fixed static device array instead of per-call allocations, so
- * n may not exceed EMPI_NOALLOC_MAX_SAMPLES (8 MiB of doubles per device,
- * held from library load until exit).  `stream` is a cudaStream_t (NULL =
- * the default stream).  The first call on a device looks the array up and
- * should happen before any stream capture.  All calls on a device share the
- * array, so calls that overlap on the GPU (other threads, other streams)
- * race and must be serialised by the caller. */
+ * device memory: a host program whose device memory is owned by another
+ * framework's pool allocator (a second allocator may find no memory left, and
+ * cudaMalloc / cudaFree synchronise the whole device, stalling that
+ * framework's streams), or a caller with a fixed device-memory budget that
+ * rules out per-call allocations.  No counterpart in the reference: the
+ * device copy of the signal and params lives in a fixed static device array
+ * instead of per-call allocations, so n may not exceed
+ * EMPI_NOALLOC_MAX_SAMPLES (8 MiB of doubles per device, held from library
+ * load until exit; larger n fails with "signalLongerThanStaticScratch", n <= 0
+ * with "invalidArgument").  `stream` is a cudaStream_t (NULL = the default
+ * stream); the call waits for it before returning, and the caller's current
+ * device is restored on every return.  The first call on a device looks up
+ * the array's device address with that device current and caches it, so it
+ * should come before any stream capture; a cudaDeviceReset of that device
+ * afterwards is not supported (the cached address would be stale).  All
+ * calls on a device share the array, so calls that overlap on the GPU (other
+ * threads, other streams) race and must be serialised by the caller. */
 #define EMPI_NOALLOC_MAX_SAMPLES (1 << 20)
 empi_status empi_subtract_atom_from_signal_noalloc(int device, void* stream, double* params,
                                                    double* samples, int n, double fs, int fit);

@@ -5,7 +5,7 @@
  * CPU checker for the CUDA engine.  Each function names the reference code it
  * restates (paths relative to the reference project).  It is pinned against
  * the reference's own sources built by oracle/Makefile (_ref/libempiref.so),
- * through tests/test_oracle_pin.py and the fixtures in tests/golden/.
+ * through tests/test_oracle.py and the fixtures in tests/golden/.
  *
  * Differences from the reference that do not change results:
  *   - maps hold one FP64 energy per (scale, t, f) instead of C complex values

@@ -31,8 +31,9 @@ class Scale(ctypes.Structure):
 
 
 def build(ref: bool = True) -> None:
-    targets = ["oracle"] + (["ref"] if ref and os.path.isdir("/root/reference/src") else [])
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    src = os.environ.get("EMPI_REFERENCE", "/root/reference")
+    targets = ["oracle"] + (["ref"] if ref and os.path.isdir(os.path.join(src, "src")) else [])
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={src}"] + targets, check=True)
 
 
 _lib = None

@@ -14,6 +14,10 @@ Writes:
                   epoch, 16384-sample windows that need folded transforms,
                   energyError 0.001 with Nfft up to 2^17), with the
                   restatement's best-to-second margins for the tie rule
+  full/*.npz      (--full) the benchmark configurations at full size: every
+                  atom of the 8-epoch MMP2 workload, 4 channels of the 32-channel
+                  MMP3 epoch, 16 of the 512 batched SMP instances, and a
+                  2^20-point energyError 0.001 case (FULL_CASES)
 """
 from __future__ import annotations
 
@@ -83,9 +87,68 @@ def scale_main():
         json.dump({"cases": out}, f, indent=1)
 
 
+# Full-size cases at the benchmark configurations, stored compactly as .npz
+# under full/ (atoms, counts, residual-energy trajectory, restatement margins).
+# name, variant, workload, workload overrides, channel subset per epoch (None =
+# all), epochs/instances, energyError, iterations, energyPercent, pinned by
+# ("reference": empi's own classes; "restatement": mp_oracle.c, used where the
+# reference's workspace does not fit in host memory)
+FULL_CASES = [
+    # MMP2 19 ch x 8 epochs x 5120 @256 Hz, 100 iterations: the bench workload, every atom
+    ("mmp2_19x8x5120", "mmp2", 1, {}, None, 8, 0.01, 100, 99.0, "reference"),
+    # MMP3 32 ch x 16384 @512 Hz, energyError 0.005: 4 channels of epoch 0 (the
+    # reference's workspace for all 32 needs ~131 GB of host memory)
+    ("mmp3_4x16384_512", "mmp3", 2, {"epochs": 1}, 4, 1, 0.005, 50, 100.0, "reference"),
+    # batched SMP: the first 16 seeded instances of the 512, first two channels each
+    ("smp_batch_16x2", "smp", 3, {"epochs": 16}, 2, 16, 0.01, 150, 99.5, "reference"),
+    # energyError 0.001 at 16384 samples @512 Hz (Nfft up to 2^20, 144 scales):
+    # 2.7e9 dictionary values per channel, ~108 GB in the reference's workspace,
+    # 22 GB in the restatement's
+    ("smp_16384_512_eps0001", "smp", 4, {"epochs": 1}, 1, 1, 0.001, 20, 100.0, "restatement"),
+]
+
+
+def full_main(names):
+    os.makedirs(os.path.join(HERE, "full"), exist_ok=True)
+    for name, variant, wl, ov, csub, nep, eps, iters, pct, pin in FULL_CASES:
+        if names and name not in names:
+            continue
+        w = synth.workload(wl, **ov)
+        rec = {"atoms": [], "counts": [], "energies": [], "margins": [], "indices": []}
+        shas = []
+        t0 = __import__("time").time()
+        for e in range(nep):
+            x = w.epochs[e] if csub is None else w.epochs[e][:, :csub]
+            x = np.ascontiguousarray(x)
+            shas.append(__import__("hashlib").sha256(x.tobytes()).hexdigest())
+            xs = x.T.astype(np.float64)
+            m = O.decompose(variant, w.fs, xs, eps, iters, pct)
+            r = O.ref_decompose(variant, w.fs, xs, eps, iters, pct) if pin == "reference" else m
+            rec["atoms"].append(r.atoms)
+            rec["counts"].append(r.natoms)
+            rec["energies"].append(r.energies)
+            rec["margins"].append(m.margins)
+            rec["indices"].append(m.indices)
+            print(name, e, list(r.natoms), f"{__import__('time').time() - t0:.0f}s", flush=True)
+        ragged = len({a.shape for a in rec["atoms"]}) > 1
+        out = {"meta": json.dumps({"name": name, "variant": variant, "workload": wl, "overrides": ov,
+                                   "channels": csub, "epochs": nep, "fs": w.fs, "energy_error": eps,
+                                   "iterations": iters, "energy_percent": pct, "pinned_by": pin,
+                                   "signal_sha_f32": shas})}
+        for k, v in rec.items():
+            if ragged:
+                for e, a in enumerate(v):
+                    out[f"{k}_{e}"] = a
+            else:
+                out[k] = np.stack(v)
+        np.savez_compressed(os.path.join(HERE, "full", name + ".npz"), **out)
+
+
 def main():
     if "--scale" in sys.argv:
         return scale_main()
+    if "--full" in sys.argv:
+        return full_main([a for a in sys.argv[1:] if not a.startswith("--")])
     if not O.ref_available():
         raise SystemExit("oracle/_ref/libempiref.so missing: run `make -C oracle ref` first")
     out = []

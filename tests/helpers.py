@@ -6,7 +6,9 @@ the best and second-best energy at that iteration is below 1e-6 (a near-tie,
 whose order the reference itself leaves to heap/OpenMP order); after an
 exempt divergence the sequences are not compared further.  Amplitude and
 modulus must agree within 1e-5 relative, phase within 1e-5 rad, residual
-energies within 1e-6 relative.
+energies within 1e-6 relative.  Every comparison reports how many atoms it
+actually compared and, by default, fails if a near-tie exemption left fewer
+than 95 % of the reference's atoms compared.
 """
 from __future__ import annotations
 
@@ -47,16 +49,25 @@ def phase_diff(a, b):
     return abs(d)
 
 
-def compare_sequences(ref_atoms, got_atoms, margins, ref_energies=None, got_energies=None, label=""):
+MIN_COMPARED = 0.95
+
+
+def compare_sequences(ref_atoms, got_atoms, margins, ref_energies=None, got_energies=None, label="",
+                      min_fraction=MIN_COMPARED):
     """ref_atoms/got_atoms: [n][6] for one channel.  margins: oracle margins per
-    iteration.  Returns the number of atoms compared; raises AssertionError."""
+    iteration.  Returns the number of atoms compared (all of them unless a
+    near-tie exemption stopped the comparison) and asserts that it is at least
+    min_fraction of the reference's atoms; raises AssertionError."""
     n = min(len(ref_atoms), len(got_atoms))
+    total = len(ref_atoms)
     for a in range(n):
         r, g = np.asarray(ref_atoms[a]), np.asarray(got_atoms[a])
         same = all(abs(r[p] - g[p]) <= 1e-9 * max(1.0, abs(r[p])) for p in (2, 3, 4))
         if not same:
             m = margins[a] if margins is not None and a < len(margins) else 0.0
             assert m < TIE_MARGIN, f"{label} atom {a}: index mismatch with margin {m:.3e}: ref {r[2:5]} got {g[2:5]}"
+            assert a >= min_fraction * total, \
+                f"{label}: near-tie at atom {a} left only {a} of {total} atoms compared"
             return a
         for p in (0, 1):
             assert abs(r[p] - g[p]) <= AMP_RTOL * abs(r[p]) + 1e-300, \

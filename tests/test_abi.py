@@ -95,3 +95,26 @@ def test_synth_workloads_are_seeded():
     assert np.array_equal(a.epochs[0], b.epochs[0])
     w = synth.workload(3, epochs=5)
     assert len(w.epochs) == 5 and all(512 <= e.shape[0] <= 16384 for e in w.epochs)
+
+
+@pytest.mark.parametrize("fs,n,eps", [(128.0, 1280, 0.01), (256.0, 5120, 0.01), (512.0, 16384, 0.001)])
+def test_error_bound_constants(fs, n, eps):
+    """The certified FP32 bound per scale: a positive FFT error constant that
+    grows with the transform's passes and the Gaussian's width, and
+    rho = 1 / (1 - expFactor) of the worst phase-dependent bin (other than
+    k = 0 and the Nyquist bin, which are real), recomputed here in FP64."""
+    geo = empi_b200.dictionary_scales(eps, fs, n)
+    bnd = empi_b200.dictionary_error_bounds(eps, fs, n)
+    assert len(bnd) == len(geo)
+    u = 2.0 ** -24
+    for (s, nfft, fcount, tcount), (bd, rho, tph, klo, khi) in zip(geo, bnd):
+        assert 0 < klo <= khi + 1 <= fcount
+        # at least the rounding of the samples and of the Gaussian (2 * 9 u per
+        # unit of the Gaussian's sum s fs + 1), at most a few thousand u per unit
+        assert 18 * u * (s * fs + 1) <= bd <= 4000 * u * (s * fs + 2)
+        nh = nfft // 2
+        others = klo > 1 or min(fcount - 1, nh - 1) > khi
+        x = s * fs / nfft
+        want = 1.0 / (1.0 - math.exp(-2 * math.pi * x * x)) if others else 1.0
+        assert rho == pytest.approx(want, rel=1e-5)
+        assert tph >= 7 * u + rho * 68 * u

@@ -251,3 +251,19 @@ def test_cli_streams_epochs_in_batches(tmp_path, variant):
     assert out_t.count("START") == 4
     # the four complete epochs are written as in the full run
     assert book.startswith(book_t) and len(book_t) < len(book)
+
+
+@pytest.mark.parametrize("variant", ["mmp1", "mmp3"])
+def test_more_than_64_channels(engine, variant):
+    """MMP1/MMP3 sum over any channel count (src/gabor.cpp:62-70): 80 channels
+    against the restatement."""
+    from empi_b200 import synth
+
+    w = synth.workload(1, epochs=1, channels=80, samples=600, seed=19)
+    x = w.epochs[0]
+    res = empi_b200.decompose_epochs(variant, [x], w.fs, 0.02, 6, 100.0, engine=engine)[0]
+    ora = O.decompose(variant, w.fs, x.T.astype(np.float64), 0.02, 6, 100.0)
+    for c in range(80):
+        compare_sequences(ora.atoms[c, : ora.natoms[c]], res.atoms[c, : res.counts[c]], ora.margins[0],
+                          ora.energies[0] if c == 0 else None, res.energies if c == 0 else None,
+                          label=f"{variant} 80ch ch{c}")

@@ -90,3 +90,26 @@ def test_subtract_fit_matches_reference_values():
     mod = np.sum(wav / nrm * x[iL:iR + 1])
     assert abs(p[0] - mod) < 1e-12 * abs(mod)
     assert abs(p[1] - mod / nrm) < 1e-12 * abs(mod / nrm)
+
+
+FULL_FIXTURES = ["mmp2_19x8x5120", "mmp3_4x16384_512"]
+
+
+@pytest.mark.parametrize("name", FULL_FIXTURES)
+def test_full_size_fixture_signals_regenerate(name):
+    """The full-size goldens (tests/golden/full/) belong to the seeded signals
+    the GPU tests regenerate: same shapes, same float32 bytes."""
+    import json
+    import os
+
+    from empi_b200 import synth
+
+    path = os.path.join(os.path.dirname(__file__), "golden", "full", name + ".npz")
+    z = np.load(path)
+    meta = json.loads(str(z["meta"]))
+    w = synth.workload(meta["workload"], **meta["overrides"])
+    for e, sha in enumerate(meta["signal_sha_f32"]):
+        x = w.epochs[e] if meta["channels"] is None else w.epochs[e][:, : meta["channels"]]
+        assert hashlib.sha256(np.ascontiguousarray(x).tobytes()).hexdigest() == sha, (name, e)
+    counts = z["counts"] if "counts" in z.files else np.concatenate([z[f"counts_{e}"] for e in range(meta["epochs"])])
+    assert np.all(np.asarray(counts) >= 1)
