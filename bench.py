@@ -114,7 +114,7 @@ def reference_arm(args):
     value = atoms / total
     sample = (f"epoch 0 of the workload per step ({w.channels}ch x {w.samples} @ {w.fs:g} Hz, "
               f"{w.variant.upper()}, {w.iterations} iterations), reference CLI built from empi src/*.cpp "
-              f"-O3 -fopenmp with the project FP64 FFT shim (FFTW absent)")
+              f"-O3 -fopenmp with the {ref_fft_label()}")
     line = {
         "impl": "reference", "metric": "atoms/s", "value": value, "unit": "atoms/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
@@ -201,7 +201,7 @@ def cpu_baseline(w):
     return {"value": atoms / dt, "unit": "atoms/s", "cores": threads, "kind": "reference",
             "sample": f"epoch 0 of the workload ({w.channels}ch x {w.samples} @ {w.fs:g} Hz, "
                       f"{w.variant.upper()}, {w.iterations} iterations, {dt:.2f} s), reference CLI from "
-                      f"empi src/*.cpp -O3 -fopenmp with the project FP64 FFT shim (FFTW absent)"}
+                      f"empi src/*.cpp -O3 -fopenmp with the {ref_fft_label()}"}
 
 
 def measured_peaks():
@@ -213,23 +213,31 @@ def measured_peaks():
 
 
 def profiled_traffic(w):
-    """DRAM bytes of one refresh fork of the headline workload, from the
-    committed ncu summary (cold-cache capture of one epoch, scaled by the
-    epochs); None for other workloads."""
-    import re
-
+    """DRAM bytes of one refresh fork of the headline workload from the
+    committed ncu figure (profiles/refresh_traffic_mmp2_19x8x5120.json);
+    None for other workloads."""
     if w.name != "mmp2-19x8x5120@256" or len(w.epochs) != 8:
         return None
     try:
-        with open(os.path.join(ROOT, "profiles", "refresh_traffic_mmp2_1epoch.md")) as f:
-            text = f.read()
-    except OSError:
+        with open(os.path.join(ROOT, "profiles", "refresh_traffic_mmp2_19x8x5120.json")) as f:
+            return float(json.load(f)["dram_bytes_per_fork"])
+    except (OSError, KeyError, ValueError):
         return None
-    one = re.search(r"dram_bytes_per_fork_one_epoch: (\d+)", text)
-    scale = re.search(r"dram_bytes_per_fork_scale_to_bench: (\d+)", text)
-    if not one or not scale:
-        return None
-    return float(one.group(1)) * float(scale.group(1))
+
+
+def host_fftw():
+    """Whether the host has FFTW3 (the reference's FFT library) installed."""
+    try:
+        out = subprocess.run(["ldconfig", "-p"], capture_output=True, text=True, timeout=10).stdout
+    except (OSError, subprocess.SubprocessError):
+        return False
+    return "libfftw3" in out
+
+
+def ref_fft_label():
+    return ("project FP64 FFT shim in place of FFTW3 (" +
+            ("FFTW3 is installed on this host, but the reference is built from its sources where they are, "
+             "against the shim" if host_fftw() else "FFTW3 absent on this host") + ")")
 
 
 def ours(args):
@@ -343,7 +351,9 @@ def ours(args):
                     "frac": achieved_gbs / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs",
                     "traffic": tr, "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum, cold "
                                                       "cache, one epoch scaled to 8 (profiles/"
-                                                      "refresh_traffic_mmp2_1epoch.md)") if tr else None,
+                                                      "refresh_traffic_mmp2_19x8x5120.json)") if tr else None,
+                    "limiter": "FP32/ALU instruction issue, not DRAM: the residual and tables are L2-resident "
+                               "(roofline_fp32 is the binding roofline)",
                     "launch_ms": per_launch_ms, "launches": st.refresh_launches,
                     "algorithmic_bytes_per_launch": bytes_per_launch}
         fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12

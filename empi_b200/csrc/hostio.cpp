@@ -3,6 +3,7 @@
 // progress protocol.  Epochs stream through the device in batches, the next
 // batch read from the file while the current one decomposes.
 #include <algorithm>
+#include <atomic>
 #include <cctype>
 #include <climits>
 #include <cmath>
@@ -348,6 +349,7 @@ void run_config(const char* configPath, const empi_engine_opts* opts) {
     const int loops = smp ? C : 1;
     std::vector<float> chanMajor;
     int epochNumber = 0;
+    bool staged = false;  // the current chunk's epochs are already on the device (batch_stage)
     while (!cur.epochs.empty()) {
         if (!eng) {
             check(empi_engine_create(opts, &eng));
@@ -358,11 +360,55 @@ void run_config(const char* configPath, const empi_engine_opts* opts) {
         const int count = (int)cur.epochs.size();
         std::vector<empi_epoch> eps;
         for (auto& e : cur.epochs) eps.push_back(empi_epoch{reader->freqSampling, C, N, e.data()});
+
+        // The progress protocol (src/empi.cpp:159, src/classes.cpp:41-48,
+        // 83) is printed in the reference's order -- epoch by epoch, MP loop
+        // by loop -- as the device advances: after every CUDA-graph chunk the
+        // loop being printed reports its atoms so far, and the next loop
+        // starts printing once it is done.  Epochs of a batch advance
+        // together, so the first epoch's lines follow the run step by step.
+        int pe = 0, pl = 0, pp = 0;
+        bool startDone = false, chanDone = false;
+        std::vector<double> en((size_t)cap);
+        auto emit = [&](bool final) {
+            while (pe < count) {
+                if (!startDone) {
+                    std::cout << "START" << '\t' << (epochNumber + pe + 1) << '\t' << C << '\t'
+                              << settings.iteration_max << '\t' << 100 * (1 - settings.residual_energy) << std::endl;
+                    startDone = true;
+                }
+                if (smp && !chanDone) {
+                    std::cout << "CHANNEL\t" << pl << std::endl;
+                    chanDone = true;
+                }
+                int it = 0, running = 0;
+                double total = 0.0;
+                check(empi::batch_loop_progress(bg.get(), pe, pl, &it, &running, &total, en.data()));
+                for (int k = pp + 1; k <= it; ++k) {
+                    const double residue = k == 1 ? total : en[(size_t)k - 2];
+                    const double energyProgress = 100.0 * (1.0 - residue / total);
+                    const double totalProgress = std::max(100.0 * (k - 1) / settings.iteration_max, energyProgress);
+                    std::cout << "ATOM\t" << (k - 1) << '\t' << atomCount << '\t' << energyProgress << '\t'
+                              << totalProgress << std::endl;
+                }
+                pp = it;
+                if (running && !final) return;
+                pp = 0;
+                chanDone = false;
+                if (++pl == loops) {
+                    pl = 0;
+                    ++pe;
+                    startDone = false;
+                }
+            }
+        };
+
         // results of this batch, filled by the worker
-        std::vector<double> atoms((size_t)count * C * cap * 6), energies((size_t)count * loops * cap),
-            totals((size_t)count * loops);
+        std::vector<double> atoms((size_t)count * C * cap * 6);
         std::vector<int> counts((size_t)count * C);
         std::exception_ptr failure;
+        std::atomic<bool> nextReady(false);
+        bool nextStaged = false;
         std::thread worker([&] {
             try {
                 if (!bg || batchEpochs != count) {
@@ -371,45 +417,39 @@ void run_config(const char* configPath, const empi_engine_opts* opts) {
                     check(empi_batch_create(eng, variant, &dict, &settings, eps.data(), count, &batch));
                     bg.reset(batch);
                     batchEpochs = count;
+                    staged = false;
                 }
-                check(empi_batch_load(bg.get(), eps.data()));
-                check(empi_batch_run(bg.get()));
-                for (int e = 0; e < count; ++e) {
+                if (!staged) check(empi_batch_load(bg.get(), eps.data()));
+                check(empi::batch_run_hooked(bg.get(), [&] {
+                    emit(false);
+                    // the next batch's host-to-device copy on the copy stream,
+                    // overlapping the rest of this run, once it has been read
+                    if (!nextStaged && nextReady.load() && (int)next.epochs.size() == count && !next.pending) {
+                        std::vector<empi_epoch> nx;
+                        for (auto& e : next.epochs) nx.push_back(empi_epoch{reader->freqSampling, C, N, e.data()});
+                        check(empi::batch_stage(bg.get(), nx.data()));
+                        nextStaged = true;
+                    }
+                }));
+                for (int e = 0; e < count; ++e)
                     check(empi_batch_atoms(bg.get(), e, cap, atoms.data() + (size_t)e * C * cap * 6,
-                                           counts.data() + (size_t)e * C, energies.data() + (size_t)e * loops * cap,
-                                           nullptr));
-                    check(empi_batch_total_energy(bg.get(), e, totals.data() + (size_t)e * loops));
-                }
+                                           counts.data() + (size_t)e * C, nullptr, nullptr));
             } catch (...) {
                 failure = std::current_exception();
             }
         });
         if (!cur.pending) readChunk(next);  // overlaps the device run
+        nextReady.store(true);
         worker.join();
         if (failure) std::rethrow_exception(failure);
+        emit(true);
+        staged = nextStaged;
 
         std::vector<uint8_t> book;
         for (int e = 0; e < count; ++e) {
             ++epochNumber;
             const double* at = atoms.data() + (size_t)e * C * cap * 6;
             const int* cn = counts.data() + (size_t)e * C;
-            const double* en = energies.data() + (size_t)e * loops * cap;
-            const double* tot = totals.data() + (size_t)e * loops;
-            // src/empi.cpp:159 and src/classes.cpp:41-48
-            std::cout << "START" << '\t' << epochNumber << '\t' << C << '\t' << settings.iteration_max << '\t'
-                      << 100 * (1 - settings.residual_energy) << std::endl;
-            for (int l = 0; l < loops; ++l) {
-                if (smp) std::cout << "CHANNEL\t" << l << std::endl;
-                const int n = cn[smp ? l : 0];
-                double residue = tot[l];
-                for (int it = 1; it <= n; ++it) {
-                    double energyProgress = 100.0 * (1.0 - residue / tot[l]);
-                    double totalProgress = std::max(100.0 * (it - 1) / settings.iteration_max, energyProgress);
-                    std::cout << "ATOM\t" << (it - 1) << '\t' << atomCount << '\t' << energyProgress << '\t'
-                              << totalProgress << std::endl;
-                    residue = en[(size_t)l * cap + it - 1];
-                }
-            }
             for (int c = 0; c < C; ++c)
                 for (int i = 0; i < N; ++i) chanMajor[(size_t)c * N + i] = cur.epochs[e][(size_t)i * C + c];
             if (epochNumber == 1) book_header(book, C, reader->freqSampling);

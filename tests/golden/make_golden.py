@@ -14,6 +14,8 @@ Writes:
                   epoch, 16384-sample windows that need folded transforms,
                   energyError 0.001 with Nfft up to 2^17), with the
                   restatement's best-to-second margins for the tie rule
+  stream_*.b/.stdout  (--cli) the reference CLI's book and progress lines
+                  for a 5-epoch, 3-channel file, MMP2 and SMP
   full/*.npz      (--full) the benchmark configurations at full size: every
                   atom of the 8-epoch MMP2 workload, 4 channels of the 32-channel
                   MMP3 epoch, 16 of the 512 batched SMP instances, and a
@@ -144,7 +146,37 @@ def full_main(names):
         np.savez_compressed(os.path.join(HERE, "full", name + ".npz"), **out)
 
 
+STREAM_CONFIG = ("energyError 0.01\nmaximalNumberOfIterations 12\nenergyPercent 99.0\nMP {mp}\n"
+                 "nameOfDataFile sig.bin\nnameOfOutputDirectory .\nsamplingFrequency 256.0\n"
+                 "numberOfChannels 3\nselectedChannels 1-3\nnumberOfSamplesInEpoch 700\n")
+
+
+def stream_signal():
+    """Five 3-channel epochs of 700 samples (workload 1, seed 11), as one file."""
+    w = synth.workload(1, epochs=5, channels=3, samples=700, seed=11)
+    return np.concatenate([e.reshape(-1) for e in w.epochs]).astype(np.float32)
+
+
+def cli_main():
+    """The reference CLI on a multi-epoch file (MMP2 and SMP): its book and
+    stdout, for the streaming tests of the GPU CLI."""
+    data = stream_signal()
+    for mp in ("MMP2", "SMP"):
+        with tempfile.TemporaryDirectory() as d:
+            data.tofile(os.path.join(d, "sig.bin"))
+            with open(os.path.join(d, "run.cfg"), "w") as f:
+                f.write(STREAM_CONFIG.format(mp=mp))
+            proc = subprocess.run([O.ref_cli(), "run.cfg"], cwd=d, capture_output=True, text=True, check=True)
+            name = f"stream_{mp.lower()}"
+            shutil.copy(os.path.join(d, f"sig_{mp.lower()[:3]}.b"), os.path.join(HERE, name + ".b"))
+            with open(os.path.join(HERE, name + ".stdout"), "w") as f:
+                f.write(proc.stdout)
+        print(name, proc.stdout.count("ATOM"), "atom lines")
+
+
 def main():
+    if "--cli" in sys.argv:
+        return cli_main()
     if "--scale" in sys.argv:
         return scale_main()
     if "--full" in sys.argv:

@@ -219,33 +219,58 @@ def test_cli_book_matches_reference(tmp_path):
         assert all(abs(a - b) <= 2e-5 * max(1.0, abs(b)) for a, b in zip(g[:5], r[:5]))
 
 
+def compare_protocol(got, ref):
+    """Progress lines (src/empi.cpp:159, src/classes.cpp:41-48, 83): the same
+    lines in the same order; ATOM percentages within print precision."""
+    g, r = got.splitlines(), ref.splitlines()
+    assert len(g) == len(r), (len(g), len(r))
+    for a, b in zip(g, r):
+        fa, fb = a.split("\t"), b.split("\t")
+        assert fa[0] == fb[0] and len(fa) == len(fb), (a, b)
+        if fa[0] == "ATOM":
+            assert fa[1:3] == fb[1:3], (a, b)
+            for x, y in zip(fa[3:], fb[3:]):
+                assert abs(float(x) - float(y)) <= 2e-4 * max(1.0, abs(float(y))), (a, b)
+        else:
+            assert a == b
+
+
 @pytest.mark.parametrize("variant", ["MMP2", "SMP"])
 def test_cli_streams_epochs_in_batches(tmp_path, variant):
-    """Epochs stream through the device in batches (gpuEpochsPerBatch): the
-    protocol lines and the book are the same bytes whatever the batch size,
-    and a truncated last epoch still ends the job with fileIsTruncated after
-    the complete epochs are written (src/empi.cpp:148-164, src/io.cpp:48-55)."""
-    from empi_b200 import synth
+    """Epochs stream through the device in batches (gpuEpochsPerBatch), the
+    next batch read from the file and copied to the device while the current
+    one runs, and the progress lines printed as the device advances.  For a
+    5-epoch, 3-channel file and every batch size the protocol lines and the
+    book match the reference CLI's own (tests/golden/stream_*), and a
+    truncated last epoch still ends the job with fileIsTruncated after the
+    complete epochs are written (src/empi.cpp:148-164, src/io.cpp:48-55)."""
+    from golden.make_golden import STREAM_CONFIG, stream_signal
 
-    w = synth.workload(1, epochs=5, channels=3, samples=700, seed=11)
-    data = np.concatenate([e.reshape(-1) for e in w.epochs]).astype(np.float32)
+    data = stream_signal()
     cli = os.path.join(os.path.dirname(empi_b200.LIB_PATH), "empi-gpu")
+    name = f"stream_{variant.lower()}"
+    ref_out = open(os.path.join(GOLDEN, name + ".stdout")).read()
+    ref_book = open(os.path.join(GOLDEN, name + ".b"), "rb").read()
+    ref_atoms = decode_book(ref_book)["atoms"]
     outs = {}
     for per, trunc in ((1, False), (2, False), (64, False), (2, True)):
         d = tmp_path / f"b{per}{'t' if trunc else ''}"
         d.mkdir()
         (data[:-5] if trunc else data).tofile(d / "sig.bin")
-        (d / "run.cfg").write_text(
-            f"energyError 0.01\nmaximalNumberOfIterations 12\nenergyPercent 99.0\nMP {variant}\n"
-            f"nameOfDataFile sig.bin\nnameOfOutputDirectory .\nsamplingFrequency {w.fs}\n"
-            f"numberOfChannels 3\nselectedChannels 1-3\nnumberOfSamplesInEpoch 700\n"
-            f"gpuEpochsPerBatch {per}\n")
+        (d / "run.cfg").write_text(STREAM_CONFIG.format(mp=variant) + f"gpuEpochsPerBatch {per}\n")
         p = subprocess.run([cli, "run.cfg"], cwd=d, capture_output=True, text=True, timeout=300)
         outs[(per, trunc)] = (p.returncode, p.stdout, (d / f"sig_{variant.lower()[:3]}.b").read_bytes())
+    for per in (1, 2, 64):
+        rc, out, book = outs[(per, False)]
+        assert rc == 0 and out.count("START") == 5
+        compare_protocol(out, ref_out)
+        assert len(book) == len(ref_book)
+        got_atoms = decode_book(book)["atoms"]
+        assert len(got_atoms) == len(ref_atoms)
+        for g, r in zip(got_atoms, ref_atoms):
+            assert all(abs(x - y) <= 2e-5 * max(1.0, abs(y)) for x, y in zip(g[:5], r[:5])), (per, g, r)
+        assert outs[(per, False)] == outs[(64, False)]  # whatever the batch size
     rc, out, book = outs[(64, False)]
-    assert rc == 0 and out.count("START") == 5 and out.rstrip().endswith("END")
-    for per in (1, 2):
-        assert outs[(per, False)] == (rc, out, book)
     rc_t, out_t, book_t = outs[(2, True)]
     assert rc_t != 0 and "ERROR\tfileIsTruncated" in out_t
     assert out_t.count("START") == 4
