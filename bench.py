@@ -258,7 +258,11 @@ def ours(args):
     w = synth.workload(args.workload, seed=1000 + args.workload + 7919 * rank, epochs=args.epochs or None,
                        iterations=args.iterations or None)
     stream = torch.cuda.Stream()
-    eng = empi_b200.Engine(device=local, stream=stream.cuda_stream)
+    from empi_b200 import autotune
+
+    # the committed autotuner cache: launch shapes tuned on a B200 per workload
+    tune_cache = autotune.DEFAULT_CACHE if os.path.exists(autotune.DEFAULT_CACHE) else None
+    eng = empi_b200.Engine(device=local, stream=stream.cuda_stream, tune_cache=tune_cache)
     settings = empi_b200.DecompositionSettings(w.iterations, 1.0 - 0.01 * w.energy_percent)
     shapes = [e.shape for e in w.epochs]
     pinned = [torch.from_numpy(e).pin_memory() for e in w.epochs]
@@ -332,7 +336,7 @@ def ours(args):
     e2e_value = units / (e2e_ms / 1e3) if e2e_ms > 0 else None
 
     # dominant kernel (k_refresh): CUDA events around every refresh launch
-    eng_t = empi_b200.Engine(device=local, stream=stream.cuda_stream, timing=True)
+    eng_t = empi_b200.Engine(device=local, stream=stream.cuda_stream, timing=True, tune_cache=tune_cache)
     bt = empi_b200.Batch(w.variant, w.energy_error, settings, shapes, w.fs, engine=eng_t)
     bt.load(host)
     for _ in range(0 if args.no_roofline else 2):
@@ -377,6 +381,8 @@ def ours(args):
             "gpu_launches": launches, "roofline": roofline, "roofline_fp32": roofline_fp32,
             "cpu_baseline": base, "clocks": clk, "atoms_per_step": atoms_per_step,
             "candidate_bins_per_atom": st.candidate_bins / max(1, st.atoms),
+            "launch_shape": {"transform_cap": st.transform_cap, "iterations_per_graph": st.iterations_per_graph,
+                             "wide_mask": st.wide_mask, "tuned": bool(st.tuned)},
         }
         print(json.dumps(line))
     batch.close()

@@ -42,7 +42,7 @@ _VARIANTS = {"smp": SMP, "mmp1": MMP1, "mmp2": MMP2, "mmp3": MMP3}
 class EngineOpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("stream", ctypes.c_void_p), ("transform_cap", ctypes.c_int),
                 ("candidate_band", ctypes.c_double), ("candidate_capacity", ctypes.c_int),
-                ("iterations_per_graph", ctypes.c_int), ("timing", ctypes.c_int)]
+                ("iterations_per_graph", ctypes.c_int), ("timing", ctypes.c_int), ("tune_cache", ctypes.c_char_p)]
 
 
 class Dictionary(ctypes.Structure):
@@ -64,7 +64,9 @@ class BatchStats(ctypes.Structure):
                 ("windows", ctypes.c_longlong), ("fft_flops", ctypes.c_double),
                 ("algorithmic_bytes", ctypes.c_double), ("refresh_ms", ctypes.c_double),
                 ("refresh_launches", ctypes.c_int), ("kernel_launches", ctypes.c_int),
-                ("candidate_bins", ctypes.c_int), ("run_ms", ctypes.c_double)]
+                ("candidate_bins", ctypes.c_int), ("run_ms", ctypes.c_double), ("transform_cap", ctypes.c_int),
+                ("iterations_per_graph", ctypes.c_int), ("wide_mask", ctypes.c_int), ("tuned", ctypes.c_int),
+                ("sizes_mask", ctypes.c_int)]
 
 
 EXPORTS = [
@@ -75,7 +77,7 @@ EXPORTS = [
     "empi_subtract_atom_from_signal", "empi_batch_create", "empi_batch_destroy", "empi_batch_load",
     "empi_batch_run", "empi_batch_atoms", "empi_batch_total_energy", "empi_batch_get_stats",
     "empi_decompose", "empi_run_config", "empi_book_write", "empi_subtract_atom_from_signal_noalloc",
-    "empi_dictionary_error_bounds",
+    "empi_dictionary_error_bounds", "empi_tune_lookup",
 ]
 
 _lib = None
@@ -105,6 +107,8 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
                                          dp, ip, ip, ip, ip]
     L.empi_dictionary_error_bounds.argtypes = [ctypes.POINTER(Dictionary), ctypes.c_double, ctypes.c_int,
                                                ctypes.c_int, fp, fp, fp, ip, ip, ip]
+    L.empi_tune_lookup.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                   ctypes.c_double, ip, ip, ip]
     L.empi_workspace_create.argtypes = [vp, ctypes.POINTER(Dictionary), ctypes.c_double, ctypes.c_int,
                                         ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
     L.empi_workspace_destroy.argtypes = [vp]
@@ -167,7 +171,7 @@ class Engine:
 
     def __init__(self, device: int = 0, stream: int | None = None, transform_cap: int = 0,
                  candidate_band: float = 0.0, candidate_capacity: int = 0, iterations_per_graph: int = 0,
-                 timing: bool = False):
+                 timing: bool = False, tune_cache: str | None = None):
         L = load_library()
         o = EngineOpts()
         L.empi_engine_opts_default(ctypes.byref(o))
@@ -182,6 +186,7 @@ class Engine:
         if iterations_per_graph:
             o.iterations_per_graph = iterations_per_graph
         o.timing = int(timing)
+        o.tune_cache = os.fsencode(tune_cache) if tune_cache else None
         h = ctypes.c_void_p()
         _check(L.empi_engine_create(ctypes.byref(o), ctypes.byref(h)))
         self.handle = h
@@ -279,6 +284,21 @@ def dictionary_error_bounds(energyError, freqSampling, sampleCount, scaleMin=0.0
                                           bd.ctypes.data_as(fp), rho.ctypes.data_as(fp), tph.ctypes.data_as(fp),
                                           _ip(klo), _ip(khi), ctypes.byref(n)))
     return [(float(bd[i]), float(rho[i]), float(tph[i]), int(klo[i]), int(khi[i])) for i in range(n.value)]
+
+
+def tune_lookup(path, mode, channels, fs, samples, energy_error):
+    """(transform_cap, iterations_per_graph, wide_mask) of the tune cache's
+    entry for a workload, or None (empi_tune_lookup; no GPU needed)."""
+    L = load_library()
+    cap, k, wide = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    st = L.empi_tune_lookup(os.fsencode(path), int(mode), int(channels), float(fs), int(samples),
+                            float(energy_error), ctypes.byref(cap), ctypes.byref(k), ctypes.byref(wide))
+    if st != 0:
+        msg = (L.empi_last_error() or b"").decode()
+        if msg == "noTunedEntry":
+            return None
+        raise EmpiError(st, msg)
+    return cap.value, k.value, wide.value
 
 
 # ---------------------------------------------------------------- workspace seam

@@ -24,13 +24,15 @@ BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
                      "--expt-relaxed-constexpr", "-diag-suppress", "177"]
-SOURCES = ["engine.cu", "geometry.cpp", "hostio.cpp"]
+SOURCES = ["engine.cu", "refresh_single.cu", "refresh_mmp1.cu", "refresh_mmp3.cu", "geometry.cpp", "hostio.cpp",
+           "tune.cpp"]
 # Device code of the engine: single-precision math with approximate division,
 # square root and exp2 and flush-to-zero (the FP32 energy maps; FP64 code is
 # unaffected).  The FP32 maps only rank candidates: every bin within 1e-4 of
 # the maximum is re-scored in FP64, and the parity tests bound the map error.
 ENGINE_FLAGS = ["--use_fast_math"]
-HEADERS = ["fft.cuh", "kernels.cuh", "refresh.cuh", "plan.hpp", "geometry.hpp", "engine.hpp"]
+HEADERS = ["fft.cuh", "common.cuh", "kernels.cuh", "refresh.cuh", "refresh_kernels.hpp", "plan.hpp", "geometry.hpp",
+           "engine.hpp", "tune.hpp"]
 
 
 def nvcc() -> str:
@@ -66,7 +68,9 @@ def build(force: bool = False, verbose: bool = False, checked: bool = False) -> 
     cc = nvcc()
     ccbin = ["-ccbin", host_cxx()]
     if force or _stale(lib, deps):
-        objs = []
+        from concurrent.futures import ThreadPoolExecutor
+
+        objs, cmds = [], []
         for src in SOURCES:
             obj = os.path.join(bdir, src + ".o")
             cmd = [cc] + ccbin + NVCC_FLAGS + ENGINE_FLAGS + extra + ["-c", os.path.join(CSRC, src), "-o", obj]
@@ -74,8 +78,14 @@ def build(force: bool = False, verbose: bool = False, checked: bool = False) -> 
                 cmd = [cc] + ccbin + ["-x", "cu"] + NVCC_FLAGS + extra + ["-c", os.path.join(CSRC, src), "-o", obj]
             if verbose:
                 print(" ".join(cmd))
-            subprocess.run(cmd, check=True)
+            cmds.append(cmd)
             objs.append(obj)
+        # the translation units compile in parallel (the refresh kernels of each
+        # variant mode are the slow ones)
+        with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as pool:
+            for r in pool.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds):
+                if r.returncode != 0:
+                    raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
         tmp = lib + ".tmp"
         cmd = [cc] + ccbin + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs
         subprocess.run(cmd, check=True)

@@ -16,6 +16,8 @@
 #include "engine.hpp"
 #include "geometry.hpp"
 #include "kernels.cuh"
+#include "refresh_kernels.hpp"
+#include "tune.hpp"
 
 using namespace empi;
 
@@ -73,7 +75,7 @@ extern "C" const char* empi_status_string(empi_status st) {
 
 // ------------------------------------------------------------ engine
 
-constexpr int kSizes = 13;  // sub-FFT sizes 2^0 .. 2^12, one refresh kernel each
+constexpr int kSizes = kRefreshSizes;  // sub-FFT sizes 2^0 .. 2^12, one refresh kernel each
 
 struct empi_engine {
     empi_engine_opts opts;
@@ -84,6 +86,8 @@ struct empi_engine {
     float2* tw = nullptr;
     cudaStream_t aux[kSizes] = {};     // branches of the per-size refresh fork
     cudaEvent_t fork = nullptr, join[kSizes] = {};
+    RefreshKernels rk[3];              // SMP / MMP2 sum, MMP1, MMP3
+    std::string tune_cache;            // autotuner cache file ("" = none)
 };
 
 extern "C" void empi_engine_opts_default(empi_engine_opts* o) {
@@ -142,6 +146,11 @@ extern "C" empi_status empi_engine_create(const empi_engine_opts* opts, empi_eng
     }
     CUDA_TRY(cudaMalloc(&e->tw, sizeof(float2) * 2 * kTwN));
     CUDA_TRY(cudaMemcpy(e->tw, tw.data(), sizeof(float2) * 2 * kTwN, cudaMemcpyHostToDevice));
+    refresh_kernels_single(e->rk[0]);
+    refresh_kernels_mmp1(e->rk[1]);
+    refresh_kernels_mmp3(e->rk[2]);
+    if (e->opts.tune_cache) e->tune_cache = e->opts.tune_cache;
+    e->opts.tune_cache = nullptr;  // the engine keeps its own copy
     CUDA_TRY(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
     for (int i = 0; i < kSizes; ++i) {
         CUDA_TRY(cudaStreamCreateWithFlags(&e->aux[i], cudaStreamNonBlocking));
@@ -225,6 +234,20 @@ extern "C" empi_status empi_dictionary_error_bounds(const empi_dictionary* d, do
     return ok();
 }
 
+extern "C" empi_status empi_tune_lookup(const char* path, int mode, int channels, double fs, int samples,
+                                        double energy_error, int* transform_cap, int* iterations_per_graph,
+                                        int* wide_mask) {
+    if (!path) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    TuneParams tp;
+    std::string err;
+    if (!tune_lookup(path, TuneKey{mode, channels, fs, samples, energy_error}, tp, err))
+        return fail(EMPI_ERR_CONFIG, err);
+    if (transform_cap) *transform_cap = tp.transform_cap;
+    if (iterations_per_graph) *iterations_per_graph = tp.iterations_per_graph;
+    if (wide_mask) *wide_mask = tp.wide_mask;
+    return ok();
+}
+
 // ------------------------------------------------------------ batch state
 
 namespace {
@@ -296,7 +319,12 @@ struct empi_batch {
     void* collect_fn = nullptr;
 
     BatchDev dev{};
-    int refresh_grid = 0, collect_grid = 0, tree_grid = 0, rescore_grid = 0;
+    int refresh_grid_lg[kSizes] = {};
+    int collect_grid = 0, tree_grid = 0, rescore_grid = 0;
+    // launch shape: largest sub-FFT, MP iterations per graph, per-size
+    // one-CTA-per-SM refresh variants, and whether the tune cache set them
+    int lcap = 4096, K = 8, wide_mask = 0;
+    bool tuned = false;
     size_t refresh_smem = 0;             // the candidate kernel's (largest layout)
     size_t refresh_smem_lg[kSizes] = {};  // per sub-FFT size
 
@@ -322,85 +350,39 @@ struct empi_batch {
 
 namespace {
 
-template <int MODE, int LG>
-void* refresh_kernel() {
-    return (void*)k_refresh<MODE, LG>;
+const RefreshKernels& kernels_of(const empi_engine* e, int mode) {
+    return mode == MODE_SINGLE ? e->rk[0] : (mode == MODE_MMP1 ? e->rk[1] : e->rk[2]);
 }
 
-template <int MODE>
-void* refresh_kernel_of(int lg) {
-    switch (lg) {
-        case 0: return refresh_kernel<MODE, 0>();
-        case 1: return refresh_kernel<MODE, 1>();
-        case 2: return refresh_kernel<MODE, 2>();
-        case 3: return refresh_kernel<MODE, 3>();
-        case 4: return refresh_kernel<MODE, 4>();
-        case 5: return refresh_kernel<MODE, 5>();
-        case 6: return refresh_kernel<MODE, 6>();
-        case 7: return refresh_kernel<MODE, 7>();
-        case 8: return refresh_kernel<MODE, 8>();
-        case 9: return refresh_kernel<MODE, 9>();
-        case 10: return refresh_kernel<MODE, 10>();
-        case 11: return refresh_kernel<MODE, 11>();
-        default: return refresh_kernel<MODE, 12>();
-    }
-}
-
-template <int MODE>
-size_t refresh_smem_of(int lg) {
-    switch (lg) {
-        case 0: return refresh_smem_bytes<MODE, 0>();
-        case 1: return refresh_smem_bytes<MODE, 1>();
-        case 2: return refresh_smem_bytes<MODE, 2>();
-        case 3: return refresh_smem_bytes<MODE, 3>();
-        case 4: return refresh_smem_bytes<MODE, 4>();
-        case 5: return refresh_smem_bytes<MODE, 5>();
-        case 6: return refresh_smem_bytes<MODE, 6>();
-        case 7: return refresh_smem_bytes<MODE, 7>();
-        case 8: return refresh_smem_bytes<MODE, 8>();
-        case 9: return refresh_smem_bytes<MODE, 9>();
-        case 10: return refresh_smem_bytes<MODE, 10>();
-        case 11: return refresh_smem_bytes<MODE, 11>();
-        default: return refresh_smem_bytes<MODE, 12>();
-    }
-}
-
-template <int MODE>
-empi_status configure_refresh(empi_batch* b) {
-    int occ = 1 << 30;
-    size_t most = 0;
+// Per sub-FFT size present in the batch: the refresh kernel (two CTAs per SM,
+// or the one-CTA 128-register variant where the tuned shape says so), its
+// shared memory, L1 carveout and a grid of SMs x resident CTAs; the collect
+// kernel runs any size, so it takes the largest layout.
+empi_status configure(empi_batch* b) {
+    const RefreshKernels& rk = kernels_of(b->eng, b->mode);
     for (int lg : b->sizes) {
-        void* fn = refresh_kernel_of<MODE>(lg);
-        const size_t smem = refresh_smem_of<MODE>(lg);
+        const int wide = (b->wide_mask >> lg) & 1;
+        void* fn = rk.refresh[lg][wide];
+        const size_t smem = rk.smem[lg];
         CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         {
-            // as much L1 as two CTAs' shared memory leaves (percent of the maximum carveout)
-            const int pct = (int)std::min<size_t>(100, (2 * (smem + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024));
+            // as much L1 as the resident CTAs' shared memory leaves (percent of the maximum carveout)
+            const size_t ctas = wide ? 1 : 2;
+            const int pct = (int)std::min<size_t>(100, (ctas * (smem + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024));
             CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
         }
         int o = 0;
         CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fn, kUnitThreads, smem));
-        occ = std::min(occ, o);
+        if (o < 1) return fail(EMPI_ERR_INTERNAL, "refreshKernelDoesNotFit");
         b->refresh_fn[lg] = fn;
         b->refresh_smem_lg[lg] = smem;
+        b->refresh_grid_lg[lg] = b->eng->sms * o;
     }
-    // the candidate path runs any size in one kernel: the largest layout
-    for (int lg = 0; lg < kSizes; ++lg) most = std::max(most, refresh_smem_of<MODE>(lg));
-    b->collect_fn = (void*)k_collect<MODE>;
-    CUDA_TRY(cudaFuncSetAttribute(b->collect_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most));
-    if (occ < 1 || occ == (1 << 30)) return fail(EMPI_ERR_INTERNAL, "refreshKernelDoesNotFit");
-    b->refresh_smem = most;
-    b->refresh_grid = b->eng->sms * occ;
+    b->collect_fn = rk.collect;
+    CUDA_TRY(cudaFuncSetAttribute(b->collect_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk.collect_smem));
+    b->refresh_smem = rk.collect_smem;
     b->collect_grid = b->eng->sms;
     return EMPI_OK;
-}
-
-empi_status configure(empi_batch* b) {
-    switch (b->mode) {
-        case MODE_SINGLE: return configure_refresh<MODE_SINGLE>(b);
-        case MODE_MMP1: return configure_refresh<MODE_MMP1>(b);
-        default: return configure_refresh<MODE_MMP3>(b);
-    }
 }
 
 // the per-size refresh kernels as parallel branches: fork from s, join into s
@@ -408,14 +390,14 @@ void launch_refresh(empi_batch* b, cudaStream_t s) {
     empi_engine* e = b->eng;
     void* args[] = {&b->dev};
     if (b->sizes.size() == 1) {
-        cudaLaunchKernel(b->refresh_fn[b->sizes[0]], dim3(b->refresh_grid), dim3(kUnitThreads), args,
+        cudaLaunchKernel(b->refresh_fn[b->sizes[0]], dim3(b->refresh_grid_lg[b->sizes[0]]), dim3(kUnitThreads), args,
                          b->refresh_smem_lg[b->sizes[0]], s);
         return;
     }
     cudaEventRecord(e->fork, s);
     for (size_t i = 0; i < b->sizes.size(); ++i) {
         cudaStreamWaitEvent(e->aux[i], e->fork, 0);
-        cudaLaunchKernel(b->refresh_fn[b->sizes[i]], dim3(b->refresh_grid), dim3(kUnitThreads), args,
+        cudaLaunchKernel(b->refresh_fn[b->sizes[i]], dim3(b->refresh_grid_lg[b->sizes[i]]), dim3(kUnitThreads), args,
                          b->refresh_smem_lg[b->sizes[i]], e->aux[i]);
         cudaEventRecord(e->join[i], e->aux[i]);
     }
@@ -470,6 +452,36 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
     b->variant = variant;
     b->settings = settings ? *settings : empi_settings{result_iters, 0.0};
     const int iters = b->settings.iteration_max;
+    // the launch shape: the engine's, or the tune cache's entry for this
+    // workload (mode, channels per MP loop, fs, samples -- 0 when uneven --,
+    // energyError)
+    b->lcap = eng->opts.transform_cap;
+    b->K = eng->opts.iterations_per_graph;
+    if (!eng->tune_cache.empty()) {
+        bool multi0 = false, even = true;
+        int loopC = -1;
+        for (int e = 0; e < count; ++e) {
+            const bool m = (variant == EMPI_MMP1 || variant == EMPI_MMP3) && epochs[e].channels > 1;
+            multi0 = multi0 || m;
+            const int lc = m ? epochs[e].channels : 1;
+            if (loopC >= 0 && lc != loopC) loopC = 0;
+            else if (loopC < 0) loopC = lc;
+            even = even && epochs[e].samples == epochs[0].samples && epochs[e].fs == epochs[0].fs;
+        }
+        TuneKey key{!multi0 ? MODE_SINGLE : (variant == EMPI_MMP1 ? MODE_MMP1 : MODE_MMP3), loopC, epochs[0].fs,
+                    even ? epochs[0].samples : 0, dict->energy_error};
+        TuneParams tp;
+        std::string terr;
+        if (tune_lookup(eng->tune_cache.c_str(), key, tp, terr)) {
+            if (tp.transform_cap >= 16 && tp.transform_cap <= 4096 && !(tp.transform_cap & (tp.transform_cap - 1)))
+                b->lcap = tp.transform_cap;
+            if (tp.iterations_per_graph > 0 && tp.iterations_per_graph <= 64) b->K = tp.iterations_per_graph;
+            b->wide_mask = tp.wide_mask & ((1 << kSizes) - 1);
+            b->tuned = true;
+        } else if (terr != "noTunedEntry") {
+            return fail(EMPI_ERR_CONFIG, terr);
+        }
+    }
     std::map<std::pair<double, int>, int> dict_of;
     bool multi = false;
     for (int e = 0; e < count; ++e) {
@@ -480,7 +492,7 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
             DictPlan dp;
             std::string err;
             if (!build_dictionary(ep.fs, ep.samples, dict->energy_error, dict->scale_min, dict->scale_max,
-                                  dict->freq_max, eng->opts.transform_cap, dp, b->scales, b->etab, &b->wgeom,
+                                  dict->freq_max, b->lcap, dp, b->scales, b->etab, &b->wgeom,
                                   &b->whf, err))
                 return fail(err == "signalFileIsTooLongForThisDecomposition" ? EMPI_ERR_SIGNAL_TOO_LONG
                                                                              : EMPI_ERR_INVALID_ARGUMENT,
@@ -741,7 +753,7 @@ empi_status grow_candidates(empi_batch* b) {
 }
 
 empi_status capture_graph(empi_batch* b) {
-    const int K = b->eng->opts.iterations_per_graph;
+    const int K = b->K;
     const bool timing = b->eng->opts.timing != 0;
     if (timing && b->ev.empty()) {
         b->ev.resize(2 * (K + 1));
@@ -881,7 +893,7 @@ empi_status batch_run_hooked(empi_batch* b, const std::function<void()>& after_c
         refresh_launches++;
     }
     const int imax = b->settings.iteration_max;
-    const int K = b->eng->opts.iterations_per_graph;
+    const int K = b->K;
     // every instance stops itself after imax atoms; a chunk in which some
     // instances stall on a candidate overflow costs at most one extra chunk
     const int max_regrows = 12;
@@ -957,6 +969,11 @@ empi_status batch_run_hooked(empi_batch* b, const std::function<void()>& after_c
     b->stats.candidate_bins = ctr[CTR_STAT_BINS];
     b->stats.run_ms = run_ms;
     b->stats.algorithmic_bytes = stats[1];
+    b->stats.transform_cap = b->lcap;
+    b->stats.iterations_per_graph = b->K;
+    b->stats.wide_mask = b->wide_mask;
+    b->stats.tuned = b->tuned ? 1 : 0;
+    for (int lg : b->sizes) b->stats.sizes_mask |= 1 << lg;
     empi_status es = check_errors(b);
     if (es != EMPI_OK) return es;
     return ok();

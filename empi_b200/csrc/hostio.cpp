@@ -337,6 +337,18 @@ void run_config(const char* configPath, const empi_engine_opts* opts) {
         }
     };
 
+    // an autotuner cache (optional key the reference ignores): tuned launch
+    // shapes for the workloads it holds
+    empi_engine_opts eopts;
+    empi_engine_opts_default(&eopts);
+    if (opts) eopts = *opts;
+    std::string tuneCache;
+    if (conf.has("gpuTuneCache")) {
+        tuneCache = conf.at("gpuTuneCache");
+        eopts.tune_cache = tuneCache.c_str();
+    }
+    opts = &eopts;
+
     Chunk cur, next;
     readChunk(cur);
     empi_engine* eng = nullptr;

@@ -12,8 +12,12 @@
 //       lanes of the window.
 // Window geometry (iL, length, centre) comes from host tables computed in FP64
 // with the reference's expressions, so the device does no per-window FP64.
-// Included from kernels.cuh.
 #pragma once
+
+#include "common.cuh"
+#include "refresh_kernels.hpp"
+
+namespace empi {
 
 constexpr int kVPT = kUnitPoints / kUnitThreads;
 constexpr int kBufFloat2 = kUnitPoints + kUnitPoints / 16 + 16;
@@ -1006,14 +1010,13 @@ __device__ __forceinline__ void collect_body(const BatchDev& b, unsigned char* s
     unit_body<LOGL, MODE, true>(b, smem, inst, j, g, t, 1, tstar);
 }
 
-#ifndef EMPI_REFRESH_MIN_BLOCKS
-#define EMPI_REFRESH_MIN_BLOCKS 2
-#endif
-
 // Refresh of one sub-FFT size: CTAs pull (instance, scale, group, t-batch)
-// units from that size's list, which the schedule filled.
-template <int MODE, int LOGL>
-__global__ void __launch_bounds__(kUnitThreads, EMPI_REFRESH_MIN_BLOCKS) k_refresh(BatchDev b) {
+// units from that size's list, which the schedule filled.  MINB = 2: two
+// CTAs per SM at 64 registers a thread (the default); MINB = 1: one CTA per SM
+// at 128 registers, without spills (the "wide" variant the autotuner may pick
+// per size).
+template <int MODE, int LOGL, int MINB>
+__global__ void __launch_bounds__(kUnitThreads, MINB) k_refresh(BatchDev b) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_unit;
     const int total = min(b.lcount[LOGL], b.lcap[LOGL]);
@@ -1073,3 +1076,35 @@ __global__ void __launch_bounds__(kUnitThreads, 1) k_collect(BatchDev b) {
         }
     }
 }
+
+// The refresh and collect kernels of one variant mode, with their shared
+// memory, for the engine (filled in that mode's translation unit).
+template <int MODE, int LG>
+void fill_refresh_size(RefreshKernels& rk) {
+    rk.refresh[LG][0] = (void*)k_refresh<MODE, LG, 2>;
+    rk.refresh[LG][1] = (void*)k_refresh<MODE, LG, 1>;
+    rk.smem[LG] = refresh_smem_bytes<MODE, LG>();
+}
+
+template <int MODE>
+void fill_refresh_kernels(RefreshKernels& rk) {
+    fill_refresh_size<MODE, 0>(rk);
+    fill_refresh_size<MODE, 1>(rk);
+    fill_refresh_size<MODE, 2>(rk);
+    fill_refresh_size<MODE, 3>(rk);
+    fill_refresh_size<MODE, 4>(rk);
+    fill_refresh_size<MODE, 5>(rk);
+    fill_refresh_size<MODE, 6>(rk);
+    fill_refresh_size<MODE, 7>(rk);
+    fill_refresh_size<MODE, 8>(rk);
+    fill_refresh_size<MODE, 9>(rk);
+    fill_refresh_size<MODE, 10>(rk);
+    fill_refresh_size<MODE, 11>(rk);
+    fill_refresh_size<MODE, 12>(rk);
+    rk.collect = (void*)k_collect<MODE>;
+    size_t most = 0;
+    for (int lg = 0; lg < kRefreshSizes; ++lg) most = rk.smem[lg] > most ? rk.smem[lg] : most;
+    rk.collect_smem = most;
+}
+
+}  // namespace empi

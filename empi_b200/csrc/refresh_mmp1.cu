@@ -1,0 +1,10 @@
+// Refresh and collect kernels of the mmp1 variant mode (refresh.cuh), in a
+// translation unit of their own so the three modes compile in parallel.
+#include "refresh.cuh"
+#include "refresh_kernels.hpp"
+
+namespace empi {
+
+void refresh_kernels_mmp1(RefreshKernels& rk) { fill_refresh_kernels<MODE_MMP1>(rk); }
+
+}  // namespace empi

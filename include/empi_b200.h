@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define EMPI_B200_ABI_VERSION 1
+#define EMPI_B200_ABI_VERSION 2
 
 typedef enum {
     EMPI_OK = 0,
@@ -73,6 +73,9 @@ typedef struct {
                                 (0 = default); the buffers grow on demand */
     int iterations_per_graph;/* MP iterations per CUDA-graph launch; 0 = default */
     int timing;              /* nonzero: record CUDA events around every refresh launch */
+    const char* tune_cache;  /* autotuner cache file (empi_b200/autotune.py) or NULL: batches
+                                whose workload it holds take its tuned sub-FFT cap, iterations
+                                per graph and per-size refresh variants (copied at creation) */
 } empi_engine_opts;
 
 void empi_engine_opts_default(empi_engine_opts* opts);
@@ -109,6 +112,16 @@ empi_status empi_dictionary_scales(const empi_dictionary* dict, double fs, int s
 empi_status empi_dictionary_error_bounds(const empi_dictionary* dict, double fs, int samples, int cap,
                                          float* bnd_d, float* rho, float* tph, int* klo, int* khi,
                                          int* count);
+
+/* Tuned launch shape for a workload from an autotuner cache file, without a
+ * GPU (no counterpart in the reference, which has no launch shapes): mode 0 =
+ * single-channel MP loops (SMP, MMP2's channel sum), 1 = MMP1, 3 = MMP3;
+ * channels per MP loop; samples 0 matches an entry tuned for uneven batches.
+ * Returns EMPI_ERR_CONFIG ("noTunedEntry", "invalidTuneCache") when there is
+ * none. */
+empi_status empi_tune_lookup(const char* path, int mode, int channels, double fs, int samples,
+                             double energy_error, int* transform_cap, int* iterations_per_graph,
+                             int* wide_mask);
 
 /* -------------------------------------------------- workspace (the seam) */
 
@@ -225,6 +238,11 @@ typedef struct {
     int kernel_launches;      /* kernels launched by the last run */
     int candidate_bins;       /* FP64 re-scored bins over the last run */
     double run_ms;            /* device time of the last empi_batch_run */
+    int transform_cap;        /* launch shape in use: largest sub-FFT, */
+    int iterations_per_graph; /* MP iterations per graph launch, */
+    int wide_mask;            /* sub-FFT sizes (bit log2 L) with one 128-register CTA per SM, */
+    int tuned;                /* and whether it came from the tune cache */
+    int sizes_mask;           /* sub-FFT sizes (bit log2 L) the batch's dictionaries use */
 } empi_batch_stats;
 
 empi_status empi_batch_get_stats(empi_batch* batch, empi_batch_stats* stats);

@@ -28,7 +28,7 @@ def test_library_exports_every_declared_function():
     for n in names:
         assert hasattr(L, n), n
     assert set(names) == set(empi_b200.EXPORTS)
-    assert L.empi_abi_version() == 1
+    assert L.empi_abi_version() == 2
 
 
 @pytest.mark.parametrize("fs,n,eps", [(128.0, 1280, 0.01), (256.0, 5120, 0.01), (512.0, 16384, 0.005),
@@ -118,3 +118,41 @@ def test_error_bound_constants(fs, n, eps):
         want = 1.0 / (1.0 - math.exp(-2 * math.pi * x * x)) if others else 1.0
         assert rho == pytest.approx(want, rel=1e-5)
         assert tph >= 7 * u + rho * 68 * u
+
+
+def test_tune_cache_lookup(tmp_path):
+    """The engine's reader of the autotuner's cache (empi_tune_lookup):
+    entries match on (mode, channels, fs, samples, energyError); samples 0 is
+    the entry of uneven batches; unknown keys and string values are skipped."""
+    from empi_b200 import autotune
+
+    path = tmp_path / "cache.json"
+    e1 = dict(mode=0, channels=1, fs=256.0, samples=5120, energy_error=0.01, transform_cap=2048,
+              iterations_per_graph=16, wide_mask=5, gpu="NVIDIA B200", tuned_ms=1.5)
+    e2 = dict(mode=0, channels=1, fs=256.0, samples=0, energy_error=0.01, transform_cap=1024,
+              iterations_per_graph=4, wide_mask=0, variant="smp")
+    autotune.write_cache(str(path), e1)
+    autotune.write_cache(str(path), e2)
+    autotune.write_cache(str(path), dict(e1, wide_mask=4))  # replaces e1
+    assert empi_b200.tune_lookup(str(path), 0, 1, 256.0, 5120, 0.01) == (2048, 16, 4)
+    assert empi_b200.tune_lookup(str(path), 0, 1, 256.0, 0, 0.01) == (1024, 4, 0)
+    assert empi_b200.tune_lookup(str(path), 3, 1, 256.0, 5120, 0.01) is None
+    assert empi_b200.tune_lookup(str(path), 0, 1, 256.0, 5120, 0.02) is None
+    bad = tmp_path / "bad.json"
+    bad.write_text('{"entries": [{"mode": 0,, }]}')
+    with pytest.raises(empi_b200.EmpiError) as ei:
+        empi_b200.tune_lookup(str(bad), 0, 1, 256.0, 5120, 0.01)
+    assert ei.value.message == "invalidTuneCache"
+    with pytest.raises(empi_b200.EmpiError):
+        empi_b200.tune_lookup(str(tmp_path / "missing.json"), 0, 1, 256.0, 5120, 0.01)
+
+
+def test_tune_workload_key():
+    from empi_b200 import autotune, synth
+
+    w = synth.workload(1, epochs=2, channels=3, samples=700, seed=1)
+    assert autotune.workload_key("mmp2", w.epochs, w.fs, 0.01) == dict(mode=0, channels=1, fs=256.0, samples=700,
+                                                                     energy_error=0.01)
+    assert autotune.workload_key("mmp3", w.epochs, w.fs, 0.01)["mode"] == 3
+    u = synth.workload(3, epochs=3)
+    assert autotune.workload_key("smp", u.epochs, u.fs, 0.01)["samples"] == 0
