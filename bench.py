@@ -49,6 +49,9 @@ def parse():
     p.add_argument("--epochs", type=int, default=0, help="decompose only the first E epochs (instances)")
     p.add_argument("--iterations", type=int, default=0, help="override the iteration count")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--scaling", default="weak", choices=["weak", "strong"],
+                   help="weak: every rank decomposes its own copy of the workload (the default); strong: one "
+                        "workload split across the ranks by estimated cost (empi_b200.shard)")
     p.add_argument("--no-roofline", action="store_true")
     return p.parse_args()
 
@@ -127,7 +130,7 @@ def reference_arm(args):
     print(json.dumps(line))
 
 
-def workload_config(w, world):
+def workload_config(w, world, scaling="weak"):
     if len({e.shape for e in w.epochs}) > 1:
         shape = (f"{len(w.epochs)} uneven instances ({sum(e.shape[1] for e in w.epochs)} channels, "
                  f"{min(e.shape[0] for e in w.epochs)}-{max(e.shape[0] for e in w.epochs)} samples)")
@@ -138,7 +141,7 @@ def workload_config(w, world):
                         f"energyPercent {w.energy_percent}",
             "variant": w.variant, "channels": w.channels, "epochs": len(w.epochs), "samples": w.samples,
             "fs": w.fs, "energy_error": w.energy_error, "iterations": w.iterations,
-            "energy_percent": w.energy_percent, "parallelism": f"instances x{world} (weak)",
+            "energy_percent": w.energy_percent, "parallelism": f"instances x{world} ({scaling})",
             "l2": "256 MiB buffer written between timed steps (inputs are smaller than L2)"}
 
 
@@ -255,8 +258,19 @@ def ours(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-    w = synth.workload(args.workload, seed=1000 + args.workload + 7919 * rank, epochs=args.epochs or None,
-                       iterations=args.iterations or None)
+    if args.scaling == "strong":
+        # one job for all ranks, its epochs split by estimated cost (no collective on the data path)
+        from empi_b200 import shard
+
+        w = synth.workload(args.workload, epochs=args.epochs or None, iterations=args.iterations or None)
+        costs = [shard.epoch_cost(e.shape, w.fs, w.energy_error, w.iterations, w.variant) for e in w.epochs]
+        job_epochs = len(w.epochs)
+        w.epochs = [w.epochs[i] for i in shard.partition(costs, world)[rank]]
+        if not w.epochs:
+            raise SystemExit(f"strong scaling: {job_epochs} epochs for {world} ranks leaves rank {rank} idle")
+    else:
+        w = synth.workload(args.workload, seed=1000 + args.workload + 7919 * rank, epochs=args.epochs or None,
+                           iterations=args.iterations or None)
     stream = torch.cuda.Stream()
     from empi_b200 import autotune
 
@@ -302,7 +316,8 @@ def ours(args):
         total_ms += e0.elapsed_time(e1)
     barrier()
     clk = clocks.stop()
-    launches = batch.stats().kernel_launches
+    bs = batch.stats()  # the timed batch's last run
+    launches = bs.kernel_launches
 
     # end to end through the public API: pinned host inputs in, atoms out
     e2e_ms = 0.0
@@ -328,10 +343,13 @@ def ours(args):
     h2d = sum(e.nbytes for e in host)
 
     t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
+    n_atoms = torch.tensor([float(atoms_per_step)], dtype=torch.float64, device=f"cuda:{local}")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(n_atoms, op=dist.ReduceOp.SUM)
     total_ms, e2e_ms = float(t[0]), float(t[1])
-    units = atoms_per_step * args.steps * world
+    atoms_all_ranks = float(n_atoms[0])  # weak: world x one workload's atoms; strong: the one job's
+    units = atoms_all_ranks * args.steps
     value = units / (total_ms / 1e3)
     e2e_value = units / (e2e_ms / 1e3) if e2e_ms > 0 else None
 
@@ -375,14 +393,16 @@ def ours(args):
         line = {
             "metric": "atoms/s", "value": value, "unit": "atoms/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FFT maps) + f64 (rescore, residual, energies)",
-            "data": "synthetic", "config": workload_config(w, world),
+            "scaling": args.scaling, "vs_baseline": None,
+            "dtype": "f32 (FFT maps) + f64 (rescore, residual, energies)",
+            "data": "synthetic", "config": dict(workload_config(w, world, args.scaling),
+                                                **({"job_epochs": job_epochs} if args.scaling == "strong" else {})),
             "e2e": {"value": e2e_value, "unit": "atoms/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "roofline": roofline, "roofline_fp32": roofline_fp32,
             "cpu_baseline": base, "clocks": clk, "atoms_per_step": atoms_per_step,
-            "candidate_bins_per_atom": st.candidate_bins / max(1, st.atoms),
-            "launch_shape": {"transform_cap": st.transform_cap, "iterations_per_graph": st.iterations_per_graph,
-                             "wide_mask": st.wide_mask, "tuned": bool(st.tuned)},
+            "candidate_bins_per_atom": bs.candidate_bins / max(1, bs.atoms),
+            "launch_shape": {"transform_cap": bs.transform_cap, "iterations_per_graph": bs.iterations_per_graph,
+                             "wide_mask": bs.wide_mask, "tuned": bool(bs.tuned)},
         }
         print(json.dumps(line))
     batch.close()

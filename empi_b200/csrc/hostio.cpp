@@ -14,6 +14,7 @@
 #include <fstream>
 #include <iostream>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <sstream>
 #include <stdexcept>
@@ -347,43 +348,73 @@ void run_config(const char* configPath, const empi_engine_opts* opts) {
         tuneCache = conf.at("gpuTuneCache");
         eopts.tune_cache = tuneCache.c_str();
     }
-    opts = &eopts;
+    // GPUs: EMPI_DEVICES="0,1,..." shards every batch's epochs across one
+    // engine per listed device (contiguous, equal shares: a batch's epochs
+    // have one shape); otherwise the options' device
+    std::vector<int> devices;
+    if (const char* dv = getenv("EMPI_DEVICES")) {
+        std::stringstream ds(dv);
+        std::string tok;
+        while (std::getline(ds, tok, ','))
+            if (!tok.empty()) devices.push_back(atoi(tok.c_str()));
+    }
+    if (devices.empty()) devices.push_back(eopts.device);
+    const int D = (int)devices.size();
 
     Chunk cur, next;
     readChunk(cur);
-    empi_engine* eng = nullptr;
-    std::unique_ptr<empi_engine, void (*)(empi_engine*)> eg(nullptr, empi_engine_destroy);
-    std::unique_ptr<empi_batch, void (*)(empi_batch*)> bg(nullptr, empi_batch_destroy);
-    int batchEpochs = 0;
+    std::vector<std::unique_ptr<empi_engine, void (*)(empi_engine*)>> eg;
+    std::vector<std::unique_ptr<empi_batch, void (*)(empi_batch*)>> bg;
+    for (int d = 0; d < D; ++d) {
+        eg.emplace_back(nullptr, empi_engine_destroy);
+        bg.emplace_back(nullptr, empi_batch_destroy);
+    }
+    std::vector<int> batchEpochs(D, 0);
+    std::vector<char> staged(D, 0);  // a device's share of the current chunk is already on it
     uint64_t atomCount = 0;
     const int cap = settings.iteration_max;
     const bool smp = variant == EMPI_SMP;
     const int loops = smp ? C : 1;
     std::vector<float> chanMajor;
     int epochNumber = 0;
-    bool staged = false;  // the current chunk's epochs are already on the device (batch_stage)
     while (!cur.epochs.empty()) {
-        if (!eng) {
-            check(empi_engine_create(opts, &eng));
-            eg.reset(eng);
+        if (!eg[0]) {
+            for (int d = 0; d < D; ++d) {
+                empi_engine_opts o = eopts;
+                o.device = devices[d];
+                empi_engine* e = nullptr;
+                check(empi_engine_create(&o, &e));
+                eg[d].reset(e);
+            }
             check(empi_dictionary_size(&dict, reader->freqSampling, N, &atomCount, nullptr));
             chanMajor.resize((size_t)C * N);
         }
         const int count = (int)cur.epochs.size();
-        std::vector<empi_epoch> eps;
-        for (auto& e : cur.epochs) eps.push_back(empi_epoch{reader->freqSampling, C, N, e.data()});
+        // device d takes epochs [first[d], first[d + 1])
+        std::vector<int> first(D + 1);
+        for (int d = 0; d <= D; ++d) first[d] = (int)((long long)count * d / D);
+        auto owner = [&](int e) {
+            int d = 0;
+            while (first[d + 1] <= e) ++d;
+            return d;
+        };
 
         // The progress protocol (src/empi.cpp:159, src/classes.cpp:41-48,
         // 83) is printed in the reference's order -- epoch by epoch, MP loop
-        // by loop -- as the device advances: after every CUDA-graph chunk the
-        // loop being printed reports its atoms so far, and the next loop
-        // starts printing once it is done.  Epochs of a batch advance
-        // together, so the first epoch's lines follow the run step by step.
+        // by loop -- as the devices advance: after every CUDA-graph chunk the
+        // device holding the epoch being printed reports its atoms so far, and
+        // the next loop starts printing once it is done.  Epochs of a batch
+        // advance together, so the first epoch's lines follow the run step by
+        // step.
+        std::mutex printMutex;
         int pe = 0, pl = 0, pp = 0;
         bool startDone = false, chanDone = false;
         std::vector<double> en((size_t)cap);
-        auto emit = [&](bool final) {
+        auto emit = [&](bool final, int fromDevice) {
+            std::lock_guard<std::mutex> lock(printMutex);
             while (pe < count) {
+                const int d = owner(pe);
+                if (!final && d != fromDevice) return;  // its device's own hook prints it
                 if (!startDone) {
                     std::cout << "START" << '\t' << (epochNumber + pe + 1) << '\t' << C << '\t'
                               << settings.iteration_max << '\t' << 100 * (1 - settings.residual_energy) << std::endl;
@@ -395,7 +426,7 @@ void run_config(const char* configPath, const empi_engine_opts* opts) {
                 }
                 int it = 0, running = 0;
                 double total = 0.0;
-                check(empi::batch_loop_progress(bg.get(), pe, pl, &it, &running, &total, en.data()));
+                check(empi::batch_loop_progress(bg[d].get(), pe - first[d], pl, &it, &running, &total, en.data()));
                 for (int k = pp + 1; k <= it; ++k) {
                     const double residue = k == 1 ? total : en[(size_t)k - 2];
                     const double energyProgress = 100.0 * (1.0 - residue / total);
@@ -415,46 +446,56 @@ void run_config(const char* configPath, const empi_engine_opts* opts) {
             }
         };
 
-        // results of this batch, filled by the worker
+        // results of this batch, filled by the workers (one per device)
         std::vector<double> atoms((size_t)count * C * cap * 6);
         std::vector<int> counts((size_t)count * C);
-        std::exception_ptr failure;
+        std::vector<std::exception_ptr> failure(D);
         std::atomic<bool> nextReady(false);
-        bool nextStaged = false;
-        std::thread worker([&] {
-            try {
-                if (!bg || batchEpochs != count) {
-                    empi_batch* batch = nullptr;
-                    bg.reset();
-                    check(empi_batch_create(eng, variant, &dict, &settings, eps.data(), count, &batch));
-                    bg.reset(batch);
-                    batchEpochs = count;
-                    staged = false;
-                }
-                if (!staged) check(empi_batch_load(bg.get(), eps.data()));
-                check(empi::batch_run_hooked(bg.get(), [&] {
-                    emit(false);
-                    // the next batch's host-to-device copy on the copy stream,
-                    // overlapping the rest of this run, once it has been read
-                    if (!nextStaged && nextReady.load() && (int)next.epochs.size() == count && !next.pending) {
-                        std::vector<empi_epoch> nx;
-                        for (auto& e : next.epochs) nx.push_back(empi_epoch{reader->freqSampling, C, N, e.data()});
-                        check(empi::batch_stage(bg.get(), nx.data()));
-                        nextStaged = true;
+        std::vector<char> nextStaged(D, 0);
+        std::vector<std::thread> workers;
+        for (int d = 0; d < D; ++d) {
+            const int n = first[d + 1] - first[d];
+            if (n == 0) continue;
+            workers.emplace_back([&, d, n] {
+                try {
+                    std::vector<empi_epoch> eps;
+                    for (int e = first[d]; e < first[d + 1]; ++e)
+                        eps.push_back(empi_epoch{reader->freqSampling, C, N, cur.epochs[e].data()});
+                    if (!bg[d] || batchEpochs[d] != n) {
+                        empi_batch* batch = nullptr;
+                        bg[d].reset();
+                        check(empi_batch_create(eg[d].get(), variant, &dict, &settings, eps.data(), n, &batch));
+                        bg[d].reset(batch);
+                        batchEpochs[d] = n;
+                        staged[d] = 0;
                     }
-                }));
-                for (int e = 0; e < count; ++e)
-                    check(empi_batch_atoms(bg.get(), e, cap, atoms.data() + (size_t)e * C * cap * 6,
-                                           counts.data() + (size_t)e * C, nullptr, nullptr));
-            } catch (...) {
-                failure = std::current_exception();
-            }
-        });
-        if (!cur.pending) readChunk(next);  // overlaps the device run
+                    if (!staged[d]) check(empi_batch_load(bg[d].get(), eps.data()));
+                    check(empi::batch_run_hooked(bg[d].get(), [&] {
+                        emit(false, d);
+                        // this device's share of the next batch, copied on the
+                        // copy stream while the rest of this run goes on
+                        if (!nextStaged[d] && nextReady.load() && (int)next.epochs.size() == count && !next.pending) {
+                            std::vector<empi_epoch> nx;
+                            for (int e = first[d]; e < first[d + 1]; ++e)
+                                nx.push_back(empi_epoch{reader->freqSampling, C, N, next.epochs[e].data()});
+                            check(empi::batch_stage(bg[d].get(), nx.data()));
+                            nextStaged[d] = 1;
+                        }
+                    }));
+                    for (int e = 0; e < n; ++e)
+                        check(empi_batch_atoms(bg[d].get(), e, cap, atoms.data() + (size_t)(first[d] + e) * C * cap * 6,
+                                               counts.data() + (size_t)(first[d] + e) * C, nullptr, nullptr));
+                } catch (...) {
+                    failure[d] = std::current_exception();
+                }
+            });
+        }
+        if (!cur.pending) readChunk(next);  // overlaps the device runs
         nextReady.store(true);
-        worker.join();
-        if (failure) std::rethrow_exception(failure);
-        emit(true);
+        for (auto& t : workers) t.join();
+        for (auto& f : failure)
+            if (f) std::rethrow_exception(f);
+        emit(true, -1);
         staged = nextStaged;
 
         std::vector<uint8_t> book;

@@ -43,15 +43,24 @@ def partition(costs, world):
 
 
 def decompose_sharded(variant, epochs, fs, energy_error, iterations, energy_percent=100.0, scale_min=0.0,
-                      scale_max=math.inf, freq_max=math.inf, group=None, decompose_fn=None, costs=None):
+                      scale_max=math.inf, freq_max=math.inf, group=None, decompose_fn=None, costs=None,
+                      engine=None):
     """Decomposes `epochs` (list of (N, C) float32 arrays, identical on every
     rank) across the ranks of `group`; returns the per-epoch results in order
     on rank 0 and None elsewhere.  decompose_fn(variant, epochs, fs, ...)
-    defaults to empi_b200.decompose_epochs on this rank's GPU."""
+    defaults to empi_b200.decompose_epochs on this rank's GPU: `engine`, or
+    an engine on device LOCAL_RANK."""
+    import os
+
     import torch.distributed as dist
 
     if decompose_fn is None:
-        from empi_b200 import decompose_epochs as decompose_fn
+        import empi_b200
+
+        eng = engine or empi_b200.Engine(device=int(os.environ.get("LOCAL_RANK", "0")))
+
+        def decompose_fn(*args):
+            return empi_b200.decompose_epochs(*args, engine=eng)
     world = dist.get_world_size(group)
     rank = dist.get_rank(group)
     if costs is None:

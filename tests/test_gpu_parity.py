@@ -243,7 +243,8 @@ def test_cli_streams_epochs_in_batches(tmp_path, variant):
     5-epoch, 3-channel file and every batch size the protocol lines and the
     book match the reference CLI's own (tests/golden/stream_*), and a
     truncated last epoch still ends the job with fileIsTruncated after the
-    complete epochs are written (src/empi.cpp:148-164, src/io.cpp:48-55)."""
+    complete epochs are written (src/empi.cpp:148-164, src/io.cpp:48-55).
+    Sharding every batch across engines (EMPI_DEVICES) changes no byte."""
     from golden.make_golden import STREAM_CONFIG, stream_signal
 
     data = stream_signal()
@@ -253,13 +254,21 @@ def test_cli_streams_epochs_in_batches(tmp_path, variant):
     ref_book = open(os.path.join(GOLDEN, name + ".b"), "rb").read()
     ref_atoms = decode_book(ref_book)["atoms"]
     outs = {}
-    for per, trunc in ((1, False), (2, False), (64, False), (2, True)):
-        d = tmp_path / f"b{per}{'t' if trunc else ''}"
+    # (batch size, truncated file, EMPI_DEVICES): "0,0" shards every batch
+    # across two engines, both on the one GPU these tests get
+    runs = ((1, False, None), (2, False, None), (64, False, None), (2, True, None), (2, False, "0,0"),
+            (64, False, "0,0"))
+    for per, trunc, devs in runs:
+        d = tmp_path / f"b{per}{'t' if trunc else ''}{'d' if devs else ''}"
         d.mkdir()
         (data[:-5] if trunc else data).tofile(d / "sig.bin")
         (d / "run.cfg").write_text(STREAM_CONFIG.format(mp=variant) + f"gpuEpochsPerBatch {per}\n")
-        p = subprocess.run([cli, "run.cfg"], cwd=d, capture_output=True, text=True, timeout=300)
-        outs[(per, trunc)] = (p.returncode, p.stdout, (d / f"sig_{variant.lower()[:3]}.b").read_bytes())
+        env = dict(os.environ, **({"EMPI_DEVICES": devs} if devs else {}))
+        p = subprocess.run([cli, "run.cfg"], cwd=d, capture_output=True, text=True, timeout=300, env=env)
+        key = (per, trunc) if not devs else (per, "sharded")
+        outs[key] = (p.returncode, p.stdout, (d / f"sig_{variant.lower()[:3]}.b").read_bytes())
+    for per in (2, 64):
+        assert outs[(per, "sharded")] == outs[(64, False)], per  # sharded across engines: the same bytes
     for per in (1, 2, 64):
         rc, out, book = outs[(per, False)]
         assert rc == 0 and out.count("START") == 5
