@@ -53,6 +53,13 @@ def parse():
                    help="weak: every rank decomposes its own copy of the workload (the default); strong: one "
                         "workload split across the ranks by estimated cost (empi_b200.shard)")
     p.add_argument("--no-roofline", action="store_true")
+    p.add_argument("--proposal", choices=["net", "last_atom", "none"],
+                   help="time the block proposal too (same workload, plain and proposal back to back; the atoms "
+                        "must be identical); net uses --proposal-weights")
+    p.add_argument("--proposal-weights", default=os.path.join(ROOT, "empi_b200", "proposal_b200.bin"))
+    p.add_argument("--proposal-k", type=int, default=16)
+    p.add_argument("--proposal-probe", action="store_true",
+                   help="also measure the refresh work no certified block proposal could skip (one extra run)")
     return p.parse_args()
 
 
@@ -386,6 +393,51 @@ def ours(args):
     bt.close()
     eng_t.close()
 
+    proposal = None
+    if args.proposal:
+        # the same workload with the block proposal: device time per step, the
+        # atoms compared with the plain run's, hit rate and refresh work
+        bq = empi_b200.Batch(w.variant, w.energy_error, settings, shapes, w.fs, engine=eng)
+        bq.set_proposal(args.proposal, args.proposal_k, args.proposal_weights if args.proposal == "net" else None)
+        bq.load(host)
+        for _ in range(args.warmup):
+            bq.run()
+        pq_ms = 0.0
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            torch.cuda.synchronize()
+            bq.run()
+            pq_ms += bq.stats().run_ms
+        sq = bq.stats()
+        same = all(np.array_equal(bq.result(e).indices, batch.result(e).indices) and
+                   np.array_equal(bq.result(e).atoms, batch.result(e).atoms) for e in range(len(w.epochs)))
+        bq.close()
+        plain_ms = bs.run_ms
+        proposal = {"source": args.proposal, "k": args.proposal_k,
+                    "atoms_per_s": atoms_per_step * args.steps / (pq_ms * 1e-3),
+                    "plain_atoms_per_s_same_run": atoms_per_step / (plain_ms * 1e-3),
+                    "identical_atoms": bool(same),
+                    "hit_rate": sq.proposal_hits / max(1, sq.proposal_iterations),
+                    "refresh_flops_vs_plain": sq.fft_flops / max(bs.fft_flops, 1e-300),
+                    "weights": os.path.basename(args.proposal_weights) if args.proposal == "net" else None}
+
+    ceiling = None
+    if args.proposal_probe:
+        bp = empi_b200.Batch(w.variant, w.energy_error, settings, shapes, w.fs, engine=eng)
+        bp.probe_proposal(True)
+        bp.load(host)
+        bp.run()
+        sp = bp.stats()
+        bp.close()
+        frac = sp.probe_needed_work / max(sp.probe_dirty_work, 1e-300)
+        ceiling = {"needed_work_fraction": frac, "needed_slot_fraction":
+                   sp.probe_needed_slots / max(1, sp.probe_dirty_slots),
+                   "refresh_speedup_ceiling": 1.0 / max(frac, 1e-300),
+                   "what": "share of the refresh rule's FFT work whose upper bound, propagated through each "
+                           "subtraction without recomputing, still reached the next certified best: no exact "
+                           "block proposal could skip it (one-step bound; atoms unchanged)"}
+
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(w)
@@ -401,6 +453,7 @@ def ours(args):
             "gpu_launches": launches, "roofline": roofline, "roofline_fp32": roofline_fp32,
             "cpu_baseline": base, "clocks": clk, "atoms_per_step": atoms_per_step,
             "candidate_bins_per_atom": bs.candidate_bins / max(1, bs.atoms),
+            "proposal_ceiling": ceiling, "proposal": proposal,
             "launch_shape": {"transform_cap": bs.transform_cap, "iterations_per_graph": bs.iterations_per_graph,
                              "wide_mask": bs.wide_mask, "tuned": bool(bs.tuned)},
         }

@@ -66,7 +66,10 @@ class BatchStats(ctypes.Structure):
                 ("refresh_launches", ctypes.c_int), ("kernel_launches", ctypes.c_int),
                 ("candidate_bins", ctypes.c_int), ("run_ms", ctypes.c_double), ("transform_cap", ctypes.c_int),
                 ("iterations_per_graph", ctypes.c_int), ("wide_mask", ctypes.c_int), ("tuned", ctypes.c_int),
-                ("sizes_mask", ctypes.c_int)]
+                ("sizes_mask", ctypes.c_int), ("probe_dirty_slots", ctypes.c_longlong),
+                ("probe_needed_slots", ctypes.c_longlong), ("probe_dirty_work", ctypes.c_double),
+                ("probe_needed_work", ctypes.c_double), ("proposal_iterations", ctypes.c_int),
+                ("proposal_hits", ctypes.c_int)]
 
 
 EXPORTS = [
@@ -77,7 +80,9 @@ EXPORTS = [
     "empi_subtract_atom_from_signal", "empi_batch_create", "empi_batch_destroy", "empi_batch_load",
     "empi_batch_run", "empi_batch_atoms", "empi_batch_total_energy", "empi_batch_get_stats",
     "empi_decompose", "empi_run_config", "empi_book_write", "empi_subtract_atom_from_signal_noalloc",
-    "empi_dictionary_error_bounds", "empi_tune_lookup",
+    "empi_dictionary_error_bounds", "empi_tune_lookup", "empi_batch_probe_proposal", "empi_batch_set_proposal",
+    "empi_batch_collect_pairs", "empi_batch_pairs", "empi_proposal_parameter_count", "empi_proposal_scores",
+    "empi_proposal_gradients", "empi_proposal_train",
 ]
 
 _lib = None
@@ -130,6 +135,15 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.empi_batch_atoms.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ip, dp, ip]
     L.empi_batch_total_energy.argtypes = [vp, ctypes.c_int, dp]
     L.empi_batch_get_stats.argtypes = [vp, ctypes.POINTER(BatchStats)]
+    L.empi_batch_probe_proposal.argtypes = [vp, ctypes.c_int]
+    L.empi_batch_set_proposal.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_char_p]
+    L.empi_batch_collect_pairs.argtypes = [vp, ctypes.c_int]
+    L.empi_batch_pairs.argtypes = [vp, ctypes.c_int, fp, ip, ip]
+    L.empi_proposal_parameter_count.restype = ctypes.c_int
+    L.empi_proposal_scores.argtypes = [ctypes.c_int, fp, ctypes.c_int, fp, ctypes.c_int, fp]
+    L.empi_proposal_gradients.argtypes = [ctypes.c_int, fp, ip, ctypes.c_int, fp, fp, fp]
+    L.empi_proposal_train.argtypes = [ctypes.c_int, fp, ip, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_float, ctypes.c_float, ctypes.c_uint, fp, fp]
     L.empi_decompose.argtypes = [vp, ctypes.c_int, ctypes.POINTER(Dictionary), ctypes.POINTER(Settings),
                                  ctypes.POINTER(Epoch), ctypes.c_int, ctypes.c_int, dp, ip]
     L.empi_run_config.argtypes = [ctypes.c_char_p, ctypes.POINTER(EngineOpts)]
@@ -447,6 +461,35 @@ class Batch:
 
     def run(self):
         _check(load_library().empi_batch_run(self.handle))
+
+    def set_proposal(self, source="net", k=16, weights=None):
+        """Block proposal for later runs (empi_batch_set_proposal): source
+        "net" (weights file), "last_atom", "none" or None (off)."""
+        code = {"net": 0, "last_atom": 1, "none": 2, None: -1}[source]
+        _check(load_library().empi_batch_set_proposal(self.handle, code, int(k),
+                                                      os.fsencode(weights) if weights else None))
+
+    def collect_pairs(self, enable=True):
+        """Keep the residual spectrogram before every selection of later runs
+        (empi_batch_collect_pairs)."""
+        _check(load_library().empi_batch_collect_pairs(self.handle, int(bool(enable))))
+
+    def pairs(self):
+        """(spectrograms [n, 64, 128] float32, blocks [n] int32) of the last run."""
+        L = load_library()
+        n = ctypes.c_int()
+        _check(L.empi_batch_pairs(self.handle, 0, None, None, ctypes.byref(n)))
+        spec = np.zeros((n.value, 64, 128), np.float32)
+        blocks = np.zeros(n.value, np.int32)
+        if n.value:
+            _check(L.empi_batch_pairs(self.handle, n.value, spec.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                      _ip(blocks), ctypes.byref(n)))
+        return spec, blocks
+
+    def probe_proposal(self, enable=True):
+        """Measure, in later runs, the refresh work no certified block
+        proposal could skip (empi_batch_probe_proposal)."""
+        _check(load_library().empi_batch_probe_proposal(self.handle, int(bool(enable))))
 
     def stats(self) -> BatchStats:
         st = BatchStats()

@@ -29,8 +29,16 @@ enum Counter {
     CTR_STAT_BINS = 11,
     CTR_STALLED = 12,    // instances stalled by a candidate overflow since the last regrowth
     CTR_CHECK = 13,      // (EMPI_CHECK builds) largest code of a failed bounds check
+    CTR_PROP_ITERS = 14, // block proposal: iterations that used it
+    CTR_PROP_HITS = 15,  // ... and whose atom lay in a proposed block
     CTR_COUNT = 16
 };
+
+// Block proposal geometry: 16 scale bands (scale j of n falls in band
+// 16 j / n) x 32 time tiles (window t of tcount in tile 32 t / tcount).
+constexpr int kPropBands = 16;
+constexpr int kPropTiles = 32;
+constexpr int kProposalBlocks = kPropBands * kPropTiles;
 
 // Bounds self-checks of the data-dependent indices, compiled in with
 // -DEMPI_CHECK (a diagnostic build, not the product): a failed check records
@@ -59,6 +67,8 @@ struct InstState {
     unsigned long long best32;  // tree root: upper-bound bits << 32 | slot
     float bnorm;                // channel norm of max |residual| (the error bound's B)
     unsigned tstar;             // certified lower bound of the best exact energy (float bits)
+    unsigned lround;            // block proposal: the tree root's lower bound between the rounds
+    int pad_;
 };
 
 struct CandSlot {
@@ -96,6 +106,7 @@ struct BatchDev {
     InstState* state;
     unsigned long long* slots;
     unsigned long long* chunks;
+    unsigned* chunk_l;    // per leaf chunk: the largest certified lower bound of its slots (float bits)
     int2* dirty;        // per (i, j): t range [x, y]
     int* ij_units;      // per (i, j): exclusive unit prefix within instance (nscales + 1 per inst)
     int* ij_chunks;     // per (i, j): exclusive dirty-chunk prefix (nscales + 1 per inst)
@@ -114,6 +125,21 @@ struct BatchDev {
     float* chan_xmax;     // per (instance, channel): max |FP32 residual|
     double* stats;        // [0] reference-equivalent FFT flops, [1] algorithmic bytes, [2] slots
     float* dump;          // optional energy-map dump [f][t] of one scale
+    // proposal-ceiling probe (null unless enabled): per slot, the upper bound
+    // propagated through the last subtraction without recomputing it; totals
+    // [0] dirty slots, [1] slots whose propagated bound reaches the next
+    // certified best, [2] / [3] their reference-equivalent FFT work
+    float* prop;
+    double* probe;
+    // block proposal (null unless enabled): per instance the scores of the
+    // kProposalBlocks (scale band, time tile) blocks; per (instance, scale)
+    // the proposed t-range (hull of the top-k blocks' tiles in the scale's
+    // band) and the range the second, certified round must refresh
+    float* pscores;
+    int2* prange;
+    int2* qrange;
+    int prop_k;
+    unsigned char* stale;  // block proposal: per slot, 1 while its key holds propagated bounds
 };
 
 // ------------------------------------------------------------ helpers
@@ -195,6 +221,43 @@ __device__ __forceinline__ float2 twiddle_pow2(unsigned m, unsigned n, const flo
     float s, c;
     sincospif(-2.0f * (float)m / (float)n, &s, &c);
     return make_float2(c, s);
+}
+
+// (scale, window, group) of an instance's slot (slots are laid out scale by scale)
+__device__ __forceinline__ void slot_to_jtg(const BatchDev& b, const DictPlan& dp, long long slot, int& j, int& t,
+                                            int& g) {
+    int lo = 0, hi = dp.nscales - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (b.scales[dp.scale0 + mid].slot_base <= slot) lo = mid;
+        else hi = mid - 1;
+    }
+    j = lo;
+    const ScalePlan sp = b.scales[dp.scale0 + j];
+    const long long rel = slot - sp.slot_base;
+    t = (int)(rel / sp.G);
+    g = (int)(rel - (long long)t * sp.G);
+}
+
+// max over a CTA of 64-bit keys (valid in thread 0); red holds 32 words
+__device__ __forceinline__ unsigned long long block_max_u64(unsigned long long v, unsigned long long* red) {
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+        unsigned long long o = __shfl_down_sync(0xffffffffu, v, off);
+        v = o > v ? o : v;
+    }
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0ull;
+#pragma unroll
+        for (int off = 16; off; off >>= 1) {
+            unsigned long long o = __shfl_down_sync(0xffffffffu, v, off);
+            v = o > v ? o : v;
+        }
+    }
+    __syncthreads();
+    return v;
 }
 
 // max over a CTA of non-negative floats (ordered as their bit patterns);

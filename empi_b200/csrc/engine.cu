@@ -16,6 +16,7 @@
 #include "engine.hpp"
 #include "geometry.hpp"
 #include "kernels.cuh"
+#include "proposal.hpp"
 #include "refresh_kernels.hpp"
 #include "tune.hpp"
 
@@ -305,13 +306,21 @@ struct empi_batch {
     DevBuf<double> d_residual, d_atoms, d_energies, d_chan_energy, d_fit_atoms, d_stats;
     DevBuf<InstState> d_state;
     DevBuf<unsigned long long> d_slots, d_chunks;
+    DevBuf<unsigned> d_chunk_l;
     DevBuf<int2> d_dirty, d_crange;
     DevBuf<int> d_ij_units, d_ij_chunks, d_inst_units, d_inst_chunks, d_ctr, d_inst_bins;
     DevBuf<CandSlot> d_cslots;
     DevBuf<CandBin> d_cbins;
     DevBuf<double2> d_cbin_v;
     DevBuf<int4> d_indices;
-    DevBuf<float> d_dump;
+    DevBuf<float> d_dump, d_prop, d_pscores;
+    DevBuf<double> d_probe;
+    DevBuf<int2> d_prange, d_qrange;
+    DevBuf<unsigned char> d_stale;
+    int prop_source = -1;  // block proposal: 0 learned network, 1 last-atom heuristic, 2 none (k = 0)
+    ProposalNet net;       // the learned proposer's device weights and activations
+    DevBuf<float> d_pairs; // training-pair collection: [instance][iteration][64 x 128] spectrograms
+    bool collect = false;
     DevBuf<int4> d_units;
     DevBuf<int> d_lmeta;  // loff[16], lcap[16], lcount[16], lhead[16]
     std::vector<int> sizes;  // sub-FFT sizes (log2) present in the batch
@@ -417,6 +426,7 @@ void launch_update(empi_batch* b, int sched_mode, int only_scale, double tA, dou
     cudaMemsetAsync(b->dev.lcount, 0, sizeof(int) * 2 * 16, s);  // lcount and lhead
     k_sched_a<<<ninst, 128, 0, s>>>(b->dev, sched_mode, only_scale, tA, sA);
     k_sched_b<<<1, std::min(1024, 32 * ((ninst + 31) / 32)), 0, s>>>(b->dev);
+    if (b->dev.prop && sched_mode == SCHED_ITERATE) k_propagate<<<b->tree_grid, 256, 0, s>>>(b->dev);
     if (e0) cudaEventRecord(e0, s);
     launch_refresh(b, s);
     if (e1) cudaEventRecord(e1, s);
@@ -424,18 +434,57 @@ void launch_update(empi_batch* b, int sched_mode, int only_scale, double tA, dou
 }
 
 // candidates -> FP64 rescore -> atom
-void launch_select(empi_batch* b, cudaStream_t s) {
+void launch_select(empi_batch* b, cudaStream_t s, bool probe = false) {
     const int ninst = (int)b->insts.size();
     k_cand_slots<<<ninst, 256, 0, s>>>(b->dev);
+    if (probe && b->dev.prop) k_probe<<<b->tree_grid, 256, 0, s>>>(b->dev);
     launch_collect(b, s);
     k_rescore<<<b->rescore_grid, 512, 0, s>>>(b->dev);
     k_select<<<ninst, 128, 0, s>>>(b->dev);
 }
 
+void launch_net(empi_batch* b, cudaStream_t s) { net_run(b->net, b->dev, b->dev.pscores, s); }
+
+empi_status net_load(empi_batch* b, const char* path) {
+    std::vector<float> w(kNetParams);
+    std::string err;
+    if (!read_weights(path, w.data(), &err)) return fail(EMPI_ERR_IO, err);
+    if (!net_init(b->net, w.data(), (int)b->insts.size(), &err)) return fail(EMPI_ERR_CUDA, err);
+    return EMPI_OK;
+}
+
+// the two rounds of an iteration with a block proposal (kernels.cuh, "block
+// proposal"): the proposer scores blocks from the residual, round 1 refreshes
+// the dirty windows of the top ones, the other dirty slots get propagated
+// bounds, round 2 refreshes those still reaching the root's lower bound
+void launch_proposal_update(empi_batch* b, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+    const int ninst = (int)b->insts.size();
+    if (b->prop_source == 1) k_scores_last_atom<<<ninst, 256, 0, s>>>(b->dev);
+    else if (b->prop_source == 0) launch_net(b, s);
+    k_topk_ranges<<<ninst, 256, 0, s>>>(b->dev);
+    cudaMemsetAsync(b->dev.lcount, 0, sizeof(int) * 2 * 16, s);
+    k_sched_a<<<ninst, 128, 0, s>>>(b->dev, SCHED_ITERATE, -1, 0.0, 0.0);
+    k_sched_b<<<1, std::min(1024, 32 * ((ninst + 31) / 32)), 0, s>>>(b->dev);
+    if (e0) cudaEventRecord(e0, s);
+    launch_refresh(b, s);
+    k_propagate_stale<<<b->tree_grid, 256, 0, s>>>(b->dev);
+    k_tree<<<b->tree_grid, 256, 0, s>>>(b->dev);
+    k_root<<<ninst, 256, 0, s>>>(b->dev);
+    k_qualify<<<ninst, 256, 0, s>>>(b->dev);
+    cudaMemsetAsync(b->dev.lcount, 0, sizeof(int) * 2 * 16, s);
+    k_round2_sched<<<ninst, 128, 0, s>>>(b->dev);
+    launch_refresh(b, s);
+    if (e1) cudaEventRecord(e1, s);
+    k_tree<<<b->tree_grid, 256, 0, s>>>(b->dev);
+}
+
 void launch_iteration(empi_batch* b, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
-    launch_select(b, s);
+    // training pairs: the residual's spectrogram before each selection
+    if (b->collect) spectrogram(b->dev, b->d_pairs.p, s);
+    launch_select(b, s, true);
     k_subtract<<<(int)b->blk_ic.size(), 1024, 0, s>>>(b->dev);
-    launch_update(b, SCHED_ITERATE, -1, 0.0, 0.0, s, e0, e1);
+    if (b->dev.prange) launch_proposal_update(b, s, e0, e1);
+    else launch_update(b, SCHED_ITERATE, -1, 0.0, 0.0, s, e0, e1);
 }
 
 empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* dict, const empi_settings* settings,
@@ -598,6 +647,7 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
     CUDA_TRY(b->d_state.alloc(ninst));
     CUDA_TRY(b->d_slots.alloc(slot_off));
     CUDA_TRY(b->d_chunks.alloc(chunk_off));
+    CUDA_TRY(b->d_chunk_l.alloc(chunk_off));
     CUDA_TRY(b->d_dirty.alloc(ij_off));
     CUDA_TRY(b->d_crange.alloc(ij_off));
     CUDA_TRY(b->d_ij_units.alloc(ij_off + ninst));
@@ -631,6 +681,7 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
         CUDA_TRY(cudaMemcpyAsync(b->d_fit_map.p, b->fit_map.data(), sizeof(int2) * b->fit_map.size(),
                                  cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaMemsetAsync(b->d_chunks.p, 0, sizeof(unsigned long long) * b->d_chunks.n, s));
+    CUDA_TRY(cudaMemsetAsync(b->d_chunk_l.p, 0, sizeof(unsigned) * b->d_chunk_l.n, s));
     CUDA_TRY(cudaMemsetAsync(b->d_slots.p, 0, sizeof(unsigned long long) * b->d_slots.n, s));
     CUDA_TRY(cudaMemsetAsync(b->d_ctr.p, 0, sizeof(int) * CTR_COUNT, s));
     CUDA_TRY(cudaMemcpyAsync(b->d_lmeta.p, lmeta, sizeof(lmeta), cudaMemcpyHostToDevice, s));
@@ -665,6 +716,7 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
     d.state = b->d_state.p;
     d.slots = b->d_slots.p;
     d.chunks = b->d_chunks.p;
+    d.chunk_l = b->d_chunk_l.p;
     d.dirty = b->d_dirty.p;
     d.ij_units = b->d_ij_units.p;
     d.ij_chunks = b->d_ij_chunks.p;
@@ -878,6 +930,7 @@ empi_status batch_run_hooked(empi_batch* b, const std::function<void()>& after_c
     const bool timing = b->eng->opts.timing != 0;
     CUDA_TRY(cudaMemsetAsync(b->d_ctr.p, 0, sizeof(int) * CTR_COUNT, s));
     CUDA_TRY(cudaMemsetAsync(b->d_stats.p, 0, sizeof(double) * 4, s));
+    if (b->dev.probe) CUDA_TRY(cudaMemsetAsync(b->dev.probe, 0, sizeof(double) * 4, s));
     CUDA_TRY(cudaMemsetAsync(b->d_energies.p, 0xff, sizeof(double) * b->d_energies.n, s));  // NaN
     CUDA_TRY(cudaEventRecord(b->run_start, s));
     k_init<<<(int)b->blk_ic.size(), 256, 0, s>>>(b->dev, 1);
@@ -973,6 +1026,16 @@ empi_status batch_run_hooked(empi_batch* b, const std::function<void()>& after_c
     b->stats.iterations_per_graph = b->K;
     b->stats.wide_mask = b->wide_mask;
     b->stats.tuned = b->tuned ? 1 : 0;
+    b->stats.proposal_iterations = ctr[CTR_PROP_ITERS];
+    b->stats.proposal_hits = ctr[CTR_PROP_HITS];
+    if (b->dev.probe) {
+        double pr[4];
+        CUDA_TRY(cudaMemcpy(pr, b->dev.probe, sizeof(pr), cudaMemcpyDeviceToHost));
+        b->stats.probe_dirty_slots = (long long)pr[0];
+        b->stats.probe_needed_slots = (long long)pr[1];
+        b->stats.probe_dirty_work = pr[2];
+        b->stats.probe_needed_work = pr[3];
+    }
     for (int lg : b->sizes) b->stats.sizes_mask |= 1 << lg;
     empi_status es = check_errors(b);
     if (es != EMPI_OK) return es;
@@ -980,6 +1043,161 @@ empi_status batch_run_hooked(empi_batch* b, const std::function<void()>& after_c
 }
 
 }  // namespace empi
+
+extern "C" empi_status empi_batch_set_proposal(empi_batch* b, int source, int k, const char* weights) {
+    if (!b || source < -1 || source > 2 || k < 0 || k > kProposalBlocks || (source == 0 && !weights))
+        return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    if (source >= 0 && b->mode == MODE_MMP1) return fail(EMPI_ERR_INVALID_ARGUMENT, "proposalUnsupportedForMmp1");
+    if (source >= 0 && b->dev.prop) return fail(EMPI_ERR_INVALID_ARGUMENT, "proposalWithProbe");
+    empi_status st = set_device(b->eng);
+    if (st != EMPI_OK) return st;
+    CUDA_TRY(cudaStreamSynchronize(b->eng->stream));
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    b->prop_source = source;
+    if (source < 0) {
+        b->dev.pscores = nullptr;
+        b->dev.prange = nullptr;
+        b->dev.qrange = nullptr;
+        b->dev.stale = nullptr;
+        return ok();
+    }
+    if (source == 0) {
+        st = net_load(b, weights);
+        if (st != EMPI_OK) return st;
+    }
+    const size_t nij = b->nij;
+    if (!b->d_pscores.p) CUDA_TRY(b->d_pscores.alloc(b->insts.size() * (size_t)kProposalBlocks));
+    if (!b->d_prange.p) CUDA_TRY(b->d_prange.alloc(nij));
+    if (!b->d_qrange.p) CUDA_TRY(b->d_qrange.alloc(nij));
+    std::vector<int2> empty(nij, make_int2(0, -1)), qinit(nij, make_int2(0x7fffffff, -1));
+    CUDA_TRY(cudaMemcpy(b->d_prange.p, empty.data(), sizeof(int2) * nij, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(b->d_qrange.p, qinit.data(), sizeof(int2) * nij, cudaMemcpyHostToDevice));
+    b->dev.pscores = b->d_pscores.p;
+    b->dev.prange = b->d_prange.p;
+    b->dev.qrange = b->d_qrange.p;
+    b->dev.prop_k = source == 2 ? 0 : k;
+    if (!b->d_stale.p) CUDA_TRY(b->d_stale.alloc(b->d_slots.n));
+    CUDA_TRY(cudaMemset(b->d_stale.p, 0, b->d_stale.n));
+    b->dev.stale = b->d_stale.p;
+    return ok();
+}
+
+extern "C" empi_status empi_batch_collect_pairs(empi_batch* b, int enable) {
+    if (!b) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    empi_status st = set_device(b->eng);
+    if (st != EMPI_OK) return st;
+    CUDA_TRY(cudaStreamSynchronize(b->eng->stream));
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    if (enable && !b->d_pairs.p)
+        CUDA_TRY(b->d_pairs.alloc(b->insts.size() * (size_t)b->settings.iteration_max * kSpecSize));
+    b->collect = enable != 0;
+    return ok();
+}
+
+extern "C" empi_status empi_batch_pairs(empi_batch* b, int cap, float* spec, int* block, int* count) {
+    if (!b || !count || cap < 0 || (cap > 0 && (!spec || !block))) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    if (!b->d_pairs.p) return fail(EMPI_ERR_INVALID_ARGUMENT, "pairsNotCollected");
+    empi_status st = set_device(b->eng);
+    if (st != EMPI_OK) return st;
+    const int iters = b->settings.iteration_max;
+    std::vector<InstState> sts(b->insts.size());
+    std::vector<int4> ind((size_t)b->insts.size() * iters);
+    CUDA_TRY(cudaMemcpy(sts.data(), b->d_state.p, sizeof(InstState) * sts.size(), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(ind.data(), b->d_indices.p, sizeof(int4) * ind.size(), cudaMemcpyDeviceToHost));
+    int n = 0;
+    for (size_t i = 0; i < b->insts.size(); ++i) {
+        const DictPlan& dp = b->dicts[b->insts[i].dict];
+        for (int a = 0; a < sts[i].it; ++a, ++n) {
+            if (n >= cap) continue;
+            const int4 v = ind[i * iters + a];
+            const ScalePlan& sp = b->scales[dp.scale0 + v.x];
+            // the chosen atom's block: scale band x time tile (kernels.cuh, block proposal)
+            block[n] = (v.x * kPropBands / dp.nscales) * kPropTiles + (int)((long long)kPropTiles * v.y / sp.tcount);
+            CUDA_TRY(cudaMemcpy(spec + (size_t)n * kSpecSize, b->d_pairs.p + (i * iters + a) * (size_t)kSpecSize,
+                                sizeof(float) * kSpecSize, cudaMemcpyDeviceToHost));
+        }
+    }
+    *count = n;
+    return ok();
+}
+
+namespace {
+empi_status on_device(int device) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(EMPI_ERR_NO_DEVICE, "noCudaDevice");
+    if (device < 0 || device >= n) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidDevice");
+    CUDA_TRY(cudaSetDevice(device));
+    return EMPI_OK;
+}
+}  // namespace
+
+extern "C" empi_status empi_proposal_scores(int device, const float* spec, int n, const float* weights, int bf16,
+                                            float* scores) {
+    if (!spec || !weights || !scores || n < 0) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    empi_status st = on_device(device);
+    if (st != EMPI_OK) return st;
+    std::string err;
+    if (!net_scores(spec, n, weights, bf16, scores, &err)) return fail(EMPI_ERR_CUDA, err);
+    return ok();
+}
+
+extern "C" empi_status empi_proposal_gradients(int device, const float* spec, const int* labels, int n,
+                                               const float* weights, float* grads, float* loss) {
+    if (!spec || !labels || !weights || !grads || !loss || n <= 0)
+        return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    for (int i = 0; i < n; ++i)
+        if (labels[i] < 0 || labels[i] >= kProposalBlocks) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidLabel");
+    empi_status st = on_device(device);
+    if (st != EMPI_OK) return st;
+    std::string err;
+    if (!net_gradients(spec, labels, n, weights, grads, loss, &err)) return fail(EMPI_ERR_CUDA, err);
+    return ok();
+}
+
+extern "C" empi_status empi_proposal_train(int device, const float* spec, const int* labels, int n, int epochs,
+                                           int batch, float lr, float momentum, unsigned seed, float* weights,
+                                           float* losses) {
+    if (!spec || !labels || !weights || n <= 0 || epochs <= 0 || batch <= 0)
+        return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    for (int i = 0; i < n; ++i)
+        if (labels[i] < 0 || labels[i] >= kProposalBlocks) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidLabel");
+    empi_status st = on_device(device);
+    if (st != EMPI_OK) return st;
+    std::string err;
+    if (!net_train(spec, labels, n, epochs, batch, lr, momentum, seed, weights, losses, &err))
+        return fail(EMPI_ERR_CUDA, err);
+    return ok();
+}
+
+extern "C" int empi_proposal_parameter_count(void) { return kNetParams; }
+
+extern "C" empi_status empi_batch_probe_proposal(empi_batch* b, int enable) {
+    if (!b) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    empi_status st = set_device(b->eng);
+    if (st != EMPI_OK) return st;
+    CUDA_TRY(cudaStreamSynchronize(b->eng->stream));
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    if (enable && b->dev.prange) return fail(EMPI_ERR_INVALID_ARGUMENT, "proposalWithProbe");
+    if (enable) {
+        if (!b->d_prop.p) CUDA_TRY(b->d_prop.alloc(b->d_slots.n));
+        if (!b->d_probe.p) CUDA_TRY(b->d_probe.alloc(4));
+        b->dev.prop = b->d_prop.p;
+        b->dev.probe = b->d_probe.p;
+    } else {
+        b->dev.prop = nullptr;
+        b->dev.probe = nullptr;
+    }
+    return ok();
+}
 
 extern "C" empi_status empi_batch_atoms(empi_batch* b, int epoch, int cap, double* atoms, int* count,
                                         double* energies, int* indices) {

@@ -22,6 +22,23 @@ namespace empi {
 
 enum SchedMode { SCHED_ITERATE = 0, SCHED_INIT = 1, SCHED_ATOM = 2 };
 
+// statistics of refreshing windows lo..hi of a scale: reference-equivalent
+// FFT flops (2.5 Nfft log2 Nfft per window and channel) and compulsory bytes
+// (the FP32 residual span read once per channel, one 8-byte slot write per
+// (window, group))
+__device__ __forceinline__ void refresh_stats(const DictPlan& dp, const ScalePlan& sp, int C, int lo, int hi,
+                                              double& flops, double& bytes, double& slots) {
+    const int n = hi - lo + 1;
+    int iL0, iR0, iL1, iR1;
+    double tf;
+    window_bounds(grid_t(lo, dp.tMax, sp.tcount), sp.hw, dp.fs, dp.N, iL0, iR0, tf);
+    window_bounds(grid_t(hi, dp.tMax, sp.tcount), sp.hw, dp.fs, dp.N, iL1, iR1, tf);
+    const double lg = log2((double)sp.nfft);
+    flops += (double)n * C * 2.5 * sp.nfft * lg;
+    bytes += 4.0 * C * (double)(iR1 - iL0 + 1) + 8.0 * (double)n * sp.G;
+    slots += (double)n * sp.G;
+}
+
 // One CTA per instance.  SCHED_INIT: every window dirty (only_scale >= 0
 // restricts it to one scale).  SCHED_ITERATE: stop test on the residual energy
 // of the previous subtraction (src/classes.cpp:67-70), then the dirty range of
@@ -124,32 +141,33 @@ __global__ void k_sched_a(BatchDev b, int mode, int only_scale, double tA_in, do
             b.dirty[ip.ij_off + j] = make_int2(lo, hi);
             int c0 = 0;
             if (hi >= lo) {
-                const int n = hi - lo + 1;
-                for (int g = 0; g < sp.G; ++g) nu += group_units(n, g, sp);
-                // this scale's units go to the list of its sub-FFT size
-                int at = atomicAdd(b.lcount + sp.logL, nu);
-                const int cap = b.lcap[sp.logL];
-                int4* list = b.units + b.loff[sp.logL];
-                for (int g = 0; g < sp.G; ++g) {
-                    const int B = g >= 2 ? sp.B2 : sp.B1;
-                    for (int t0 = lo; t0 <= hi; t0 += B, ++at)
-                        if (at < cap) list[at] = make_int4(inst, j | (g << 16), t0, min(B, hi - t0 + 1));
+                // the windows refreshed now: the dirty range, or with a block
+                // proposal only its proposed part (the rest get propagated
+                // bounds and a certified second round, k_round2_sched)
+                int ulo = lo, uhi = hi;
+                if (b.prange && mode == SCHED_ITERATE) {
+                    const int2 pr = b.prange[ip.ij_off + j];
+                    ulo = max(lo, pr.x);
+                    uhi = min(hi, pr.y);
+                }
+                if (uhi >= ulo) {
+                    const int n = uhi - ulo + 1;
+                    for (int g = 0; g < sp.G; ++g) nu += group_units(n, g, sp);
+                    // this scale's units go to the list of its sub-FFT size
+                    int at = atomicAdd(b.lcount + sp.logL, nu);
+                    const int cap = b.lcap[sp.logL];
+                    int4* list = b.units + b.loff[sp.logL];
+                    for (int g = 0; g < sp.G; ++g) {
+                        const int B = g >= 2 ? sp.B2 : sp.B1;
+                        for (int t0 = ulo; t0 <= uhi; t0 += B, ++at)
+                            if (at < cap) list[at] = make_int4(inst, j | (g << 16), t0, min(B, uhi - t0 + 1));
+                    }
+                    refresh_stats(dp, sp, ip.C, ulo, uhi, st_flops, st_bytes, st_slots);
                 }
                 const long long s0 = sp.slot_base + (long long)lo * sp.G;
                 const long long s1 = sp.slot_base + (long long)(hi + 1) * sp.G - 1;
                 c0 = (int)(s0 / kChunk);
                 nc = (int)(s1 / kChunk) - c0 + 1;
-                // statistics: reference-equivalent FFT flops (2.5 Nfft log2 Nfft per
-                // window and channel) and compulsory bytes (the FP32 residual span
-                // read once per channel, one 8-byte slot write per (window, group))
-                int iL0, iR0, iL1, iR1;
-                double tf;
-                window_bounds(grid_t(lo, dp.tMax, sp.tcount), sp.hw, dp.fs, dp.N, iL0, iR0, tf);
-                window_bounds(grid_t(hi, dp.tMax, sp.tcount), sp.hw, dp.fs, dp.N, iL1, iR1, tf);
-                const double lg = log2((double)sp.nfft);
-                st_flops += (double)n * ip.C * 2.5 * sp.nfft * lg;
-                st_bytes += 4.0 * ip.C * (double)(iR1 - iL0 + 1) + 8.0 * (double)n * sp.G;
-                st_slots += (double)n * sp.G;
             }
             b.ij_crange[ip.ij_off + j] = make_int2(c0, nc);
         }
@@ -280,62 +298,300 @@ __global__ void k_tree(BatchDev b) {
         const long long s1 = min(s0 + kChunk, dp.slots);
         const unsigned long long* sl = b.slots + ip.slot_off;
         unsigned long long best = 0;
+        unsigned bestl = 0;
         for (long long s = s0 + lane; s < s1; s += 32) {
             const unsigned long long v = sl[s];
             const unsigned long long key = (v & 0xffffffff00000000ull) | (unsigned long long)(s);
             best = key > best ? key : best;
+            bestl = max(bestl, (unsigned)(v & 0xffffffffull));
         }
 #pragma unroll
         for (int off = 16; off; off >>= 1) {
             unsigned long long o = __shfl_down_sync(0xffffffffu, best, off);
             best = o > best ? o : best;
         }
-        if (lane == 0) b.chunks[ip.chunk_off + chunk] = best;
+        bestl = __reduce_max_sync(0xffffffffu, bestl);
+        if (lane == 0) {
+            b.chunks[ip.chunk_off + chunk] = best;
+            b.chunk_l[ip.chunk_off + chunk] = bestl;
+        }
     }
 }
 
-__device__ __forceinline__ unsigned long long block_max_u64(unsigned long long v, unsigned long long* red) {
-#pragma unroll
-    for (int off = 16; off; off >>= 1) {
-        unsigned long long o = __shfl_down_sync(0xffffffffu, v, off);
-        v = o > v ? o : v;
+// ------------------------------------------------------------ proposal-ceiling probe
+//
+// A block proposal may skip refreshing a window only if a bound certifies that
+// the window cannot hold the next atom.  Subtracting a * atom changes a
+// window's value X_k by at most |a| sum_n g_atom(n) g_window(n) (the atom's
+// envelope times the window's Gaussian, whatever the frequency), and
+// sqrt(energy) is a norm of X, so sqrt(U) grows by at most
+// sqrt(Kc rho) |a| (fs sA s / sqrt(sA^2 + s^2) exp(-pi (t - tA)^2 / (sA^2 + s^2)) + 1)
+// (the Gaussian product's integral plus one sample).  k_propagate keeps that
+// propagated bound for every window the plain rule refreshes; k_probe, after
+// the next iteration's candidate step, counts those whose propagated bound
+// still reaches the certified lower bound of the best value: no exact
+// proposal scheme can skip them, so their share of the refresh work bounds
+// what any proposal can save (for one step; stale bounds only grow).
+
+// per dirty slot of scale j, visited through the dirty leaf chunks like k_tree
+template <typename F>
+__device__ __forceinline__ void for_dirty_slots(const BatchDev& b, F&& f) {
+    const int lane = threadIdx.x & 31;
+    const int total = b.ctr[CTR_TOTAL_CHUNKS];
+    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int item = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); item < total; item += nwarps) {
+        const int inst = upper_index(b.inst_chunks, b.ninst, item);
+        int rem = item - b.inst_chunks[inst];
+        const InstPlan ip = b.insts[inst];
+        const DictPlan dp = b.dicts[ip.dict];
+        const int j = upper_index(b.ij_chunks + ip.ij_off + inst, dp.nscales, rem);
+        rem -= b.ij_chunks[ip.ij_off + inst + j];
+        const int chunk = b.ij_crange[ip.ij_off + j].x + rem;
+        const ScalePlan sp = b.scales[dp.scale0 + j];
+        const int2 dr = b.dirty[ip.ij_off + j];
+        const long long s0 = max((long long)chunk * kChunk, sp.slot_base + (long long)dr.x * sp.G);
+        const long long s1 = min((long long)(chunk + 1) * kChunk, sp.slot_base + (long long)(dr.y + 1) * sp.G);
+        for (long long s = s0 + lane; s < s1; s += 32) f(inst, ip, dp, sp, j, s);
     }
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0ull;
+}
+
+__global__ void k_propagate(BatchDev b) {
+    for_dirty_slots(b, [&](int inst, const InstPlan& ip, const DictPlan& dp, const ScalePlan& sp, int, long long s) {
+        const InstState& st = b.state[inst];
+        if (st.it < 1) return;
+        const double* p = b.atoms + ip.out_off + (long long)(st.it - 1) * ip.C * 6;
+        double a2 = 0.0;
+        for (int c = 0; c < ip.C; ++c) a2 += p[c * 6 + 1] * p[c * 6 + 1];
+        const double tA = p[2] / dp.fs, sA = p[3] / dp.fs;
+        const int t = (int)((s - sp.slot_base) / sp.G);
+        const double dt = grid_t(t, dp.tMax, sp.tcount) - tA;
+        const double w2 = sA * sA + sp.s * sp.s;
+        const double ov = dp.fs * sA * sp.s / sqrt(w2) * exp(-CUDART_PI * dt * dt / w2) + 1.0;
+        const double d = sqrt((double)sp.Kc * (double)fmaxf(1.0f, sp.bnd_rho)) * sqrt(a2) * ov * (1.0 + 1e-6);
+        const double u = sqrt((double)__uint_as_float((unsigned)(b.slots[ip.slot_off + s] >> 32))) + d;
+        b.prop[ip.slot_off + s] = (float)fmin(u * u, 3.0e38);
+    });
+}
+
+__global__ void k_probe(BatchDev b) {
+    __shared__ double red[4][32];
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for_dirty_slots(b, [&](int inst, const InstPlan& ip, const DictPlan& dp, const ScalePlan& sp, int, long long s) {
+        const InstState& st = b.state[inst];
+        if (st.status != ST_RUNNING || st.it < 1) return;
+        const double work = 2.5 * sp.nfft * log2((double)sp.nfft) * (ip.chan0 == -1 ? ip.C : 1) / sp.G;
+        acc[0] += 1.0;
+        acc[2] += work;
+        if (b.prop[ip.slot_off + s] >= __uint_as_float(st.tstar)) {
+            acc[1] += 1.0;
+            acc[3] += work;
+        }
+    });
 #pragma unroll
-        for (int off = 16; off; off >>= 1) {
-            unsigned long long o = __shfl_down_sync(0xffffffffu, v, off);
-            v = o > v ? o : v;
+    for (int k = 0; k < 4; ++k) {
+        double v = acc[k];
+#pragma unroll
+        for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
+        if (v != 0.0) atomicAdd(b.probe + threadIdx.x, v);
+    }
+}
+
+// ------------------------------------------------------------ block proposal
+//
+// With a proposal, an iteration's dirty windows (the reference's refresh rule)
+// are handled in two rounds.  Round 1 refreshes exactly the dirty windows in
+// the proposed blocks (k_topk_ranges -> k_sched_a).  Every other dirty slot
+// gets its bounds propagated through the subtraction without recomputing
+// (k_propagate_stale, the increment of k_propagate).  Round 2 refreshes the
+// dirty windows of every slot whose upper bound still reaches the tree root's
+// lower bound (k_root, k_qualify, k_round2_sched).  What stays stale has an
+// upper bound below a certified value and cannot be the argmax; later
+// candidate steps recompute any stale slot they consider, so the atoms are
+// the plain decomposition's.
+
+// Heuristic proposer (a baseline for the learned one): the blocks nearest, in
+// (band, tile) steps, to the block of the atom just subtracted.
+__global__ void k_scores_last_atom(BatchDev b) {
+    const int inst = blockIdx.x;
+    const InstState& st = b.state[inst];
+    const InstPlan ip = b.insts[inst];
+    const DictPlan dp = b.dicts[ip.dict];
+    int band = 0, tile = 0;
+    if (st.it >= 1) {
+        const int4 a = b.indices[(long long)inst * b.iter_max + st.it - 1];
+        const ScalePlan sp = b.scales[dp.scale0 + a.x];
+        band = a.x * kPropBands / dp.nscales;
+        tile = (int)((long long)kPropTiles * a.y / sp.tcount);
+    }
+    for (int i = threadIdx.x; i < kProposalBlocks; i += blockDim.x)
+        b.pscores[(long long)inst * kProposalBlocks + i] =
+            -(float)(abs(i / kPropTiles - band) + abs(i % kPropTiles - tile));
+}
+
+// per instance: the top prop_k blocks of the scores, then per scale the hull of
+// the selected tiles of its band as a t-range
+__global__ void k_topk_ranges(BatchDev b) {
+    __shared__ float s_sc[kProposalBlocks];
+    __shared__ unsigned s_sel[kPropBands];
+    __shared__ unsigned long long red[32];
+    const int inst = blockIdx.x;
+    const InstPlan ip = b.insts[inst];
+    const DictPlan dp = b.dicts[ip.dict];
+    for (int i = threadIdx.x; i < kProposalBlocks; i += blockDim.x) {
+        const float v = b.pscores[(long long)inst * kProposalBlocks + i];
+        s_sc[i] = v == v ? v : -3.0e38f;
+    }
+    if (threadIdx.x < kPropBands) s_sel[threadIdx.x] = 0u;
+    __syncthreads();
+    for (int r = 0; r < b.prop_k; ++r) {
+        // largest score, ties to the lowest block: order-preserving key
+        unsigned long long key = 0ull;
+        for (int i = threadIdx.x; i < kProposalBlocks; i += blockDim.x) {
+            const unsigned u = __float_as_uint(s_sc[i]);
+            const unsigned o = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+            const unsigned long long k = ((unsigned long long)o << 32) | (unsigned)(kProposalBlocks - 1 - i);
+            key = k > key ? k : key;
+        }
+        key = block_max_u64(key, red);
+        __shared__ int s_pick;
+        if (threadIdx.x == 0) {
+            s_pick = kProposalBlocks - 1 - (int)(key & 0xffffffffull);
+            s_sel[s_pick / kPropTiles] |= 1u << (s_pick % kPropTiles);
+            s_sc[s_pick] = -3.4e38f;
+        }
+        __syncthreads();
+    }
+    for (int j = threadIdx.x; j < dp.nscales; j += blockDim.x) {
+        const ScalePlan sp = b.scales[dp.scale0 + j];
+        const unsigned m = s_sel[j * kPropBands / dp.nscales];
+        int2 pr = make_int2(0, -1);
+        if (m) {
+            const long long tc = sp.tcount;
+            const int lo = __ffs(m) - 1, hi = 31 - __clz(m);
+            // window t lies in tile 32 t / tcount
+            pr.x = (int)((lo * tc + kPropTiles - 1) / kPropTiles);
+            pr.y = (int)(((hi + 1) * tc + kPropTiles - 1) / kPropTiles) - 1;
+        }
+        b.prange[ip.ij_off + j] = pr;
+    }
+}
+
+// the bound increment of a window of scale sp at t from the instance's last atom
+__device__ __forceinline__ double atom_increment(const BatchDev& b, const InstPlan& ip, const DictPlan& dp,
+                                                 const ScalePlan& sp, const InstState& st, int t) {
+    const double* p = b.atoms + ip.out_off + (long long)(st.it - 1) * ip.C * 6;
+    double a2 = 0.0;
+    for (int c = 0; c < ip.C; ++c) a2 += p[c * 6 + 1] * p[c * 6 + 1];
+    const double tA = p[2] / dp.fs, sA = p[3] / dp.fs;
+    const double dt = grid_t(t, dp.tMax, sp.tcount) - tA;
+    const double w2 = sA * sA + sp.s * sp.s;
+    const double ov = dp.fs * sA * sp.s / sqrt(w2) * exp(-CUDART_PI * dt * dt / w2) + 1.0;
+    return sqrt((double)sp.Kc * (double)fmaxf(1.0f, sp.bnd_rho)) * sqrt(a2) * ov * (1.0 + 1e-6);
+}
+
+__device__ __forceinline__ bool in_range(int2 r, int t) { return t >= r.x && t <= r.y; }
+
+__global__ void k_propagate_stale(BatchDev b) {
+    for_dirty_slots(b, [&](int inst, const InstPlan& ip, const DictPlan& dp, const ScalePlan& sp, int j, long long s) {
+        const InstState& st = b.state[inst];
+        const int t = (int)((s - sp.slot_base) / sp.G);
+        if (st.it < 1 || in_range(b.prange[ip.ij_off + j], t)) return;  // refreshed in round 1
+        const double d = atom_increment(b, ip, dp, sp, st, t);
+        const unsigned long long key = b.slots[ip.slot_off + s];
+        const double u = sqrt((double)__uint_as_float((unsigned)(key >> 32))) + d;
+        const double l = sqrt((double)__uint_as_float((unsigned)(key & 0xffffffffull))) - d;
+        const float U = __double2float_ru(fmin(u * u, 3.0e38));
+        const float L = l > 0.0 ? __double2float_rd(l * l) : 0.0f;
+        b.slots[ip.slot_off + s] = ((unsigned long long)__float_as_uint(U) << 32) | __float_as_uint(L);
+        b.stale[ip.slot_off + s] = 1;
+    });
+}
+
+// per instance: the largest certified lower bound of any slot after round 1
+__global__ void k_root(BatchDev b) {
+    __shared__ unsigned long long red[32];
+    const int inst = blockIdx.x;
+    InstState& st = b.state[inst];
+    const InstPlan ip = b.insts[inst];
+    const DictPlan dp = b.dicts[ip.dict];
+    unsigned lmax = 0;
+    for (int c = threadIdx.x; c < dp.chunks; c += blockDim.x) lmax = max(lmax, b.chunk_l[ip.chunk_off + c]);
+    const unsigned long long l = block_max_u64((unsigned long long)lmax, red);
+    if (threadIdx.x == 0) st.lround = (unsigned)l;
+}
+
+// per instance: every stale slot (propagated bounds, in this iteration's
+// dirty set or left from earlier ones) whose upper bound reaches the largest
+// certified lower bound; the tree's chunk maxima skip the chunks below it.
+// Qualifying windows widen their scale's round-2 range.
+__global__ void k_qualify(BatchDev b) {
+    const int inst = blockIdx.x;
+    const InstState& st = b.state[inst];
+    if (st.status != ST_RUNNING || st.it < 1) return;
+    const InstPlan ip = b.insts[inst];
+    const DictPlan dp = b.dicts[ip.dict];
+    const unsigned lb = st.lround;
+    const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    for (int c = threadIdx.x >> 5; c < dp.chunks; c += nwarps) {
+        if ((unsigned)(b.chunks[ip.chunk_off + c] >> 32) < lb) continue;
+        const long long s0 = (long long)c * kChunk;
+        const long long s1 = min(s0 + kChunk, dp.slots);
+        for (long long s = s0 + lane; s < s1; s += 32) {
+            if (!b.stale[ip.slot_off + s] || (unsigned)(b.slots[ip.slot_off + s] >> 32) < lb) continue;
+            int j, t, g;
+            slot_to_jtg(b, dp, s, j, t, g);
+            atomicMin(&b.qrange[ip.ij_off + j].x, t);
+            atomicMax(&b.qrange[ip.ij_off + j].y, t);
         }
     }
-    __syncthreads();
-    return v;
 }
+
+// per instance: round 2's units, the hull of the qualifying windows per scale
+__global__ void k_round2_sched(BatchDev b) {
+    const int inst = blockIdx.x;
+    const InstPlan ip = b.insts[inst];
+    const DictPlan dp = b.dicts[ip.dict];
+    double st_flops = 0.0, st_bytes = 0.0, st_slots = 0.0;
+    for (int j = threadIdx.x; j < dp.nscales; j += blockDim.x) {
+        const int2 q = b.qrange[ip.ij_off + j];
+        b.qrange[ip.ij_off + j] = make_int2(0x7fffffff, -1);
+        if (q.y < q.x) continue;
+        const ScalePlan sp = b.scales[dp.scale0 + j];
+        int nu = 0;
+        for (int g = 0; g < sp.G; ++g) nu += group_units(q.y - q.x + 1, g, sp);
+        int at = atomicAdd(b.lcount + sp.logL, nu);
+        const int cap = b.lcap[sp.logL];
+        int4* list = b.units + b.loff[sp.logL];
+        for (int g = 0; g < sp.G; ++g) {
+            const int B = g >= 2 ? sp.B2 : sp.B1;
+            for (int t0 = q.x; t0 <= q.y; t0 += B, ++at)
+                if (at < cap) list[at] = make_int4(inst, j | (g << 16), t0, min(B, q.y - t0 + 1));
+        }
+        refresh_stats(dp, sp, ip.C, q.x, q.y, st_flops, st_bytes, st_slots);
+    }
+    if (st_flops != 0.0) {
+        atomicAdd(b.stats + 0, st_flops);
+        atomicAdd(b.stats + 1, st_bytes);
+        atomicAdd(b.stats + 2, st_slots);
+    }
+}
+
 
 // ------------------------------------------------------------ candidates
 
-__device__ __forceinline__ void slot_to_jtg(const BatchDev& b, const DictPlan& dp, long long slot, int& j, int& t,
-                                            int& g) {
-    int lo = 0, hi = dp.nscales - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (b.scales[dp.scale0 + mid].slot_base <= slot) lo = mid;
-        else hi = mid - 1;
-    }
-    j = lo;
-    const ScalePlan sp = b.scales[dp.scale0 + j];
-    const long long rel = slot - sp.slot_base;
-    t = (int)(rel / sp.G);
-    g = (int)(rel - (long long)t * sp.G);
-}
 
 // One CTA per instance: the root of the tournament tree (the slot with the
-// largest certified upper bound U), whose certified lower bound L is a lower
-// bound of the best exact energy; every slot whose U reaches it is a candidate
-// (a warp per qualifying leaf chunk), and the largest L among the candidates
-// becomes the instance's threshold tstar for the bins (k_collect).  No slot
+// largest certified upper bound U) and the largest certified lower bound L of
+// any slot (per leaf chunk in chunk_l), a lower bound of the best exact
+// energy; every slot whose U reaches it is a candidate (a warp per qualifying
+// leaf chunk), and the largest L among the candidates becomes the instance's
+// threshold tstar for the bins (k_collect).  No slot
 // outside the candidates can hold the exact maximum, whatever the FP32 error.
 __global__ void k_cand_slots(BatchDev b) {
     __shared__ unsigned long long red[32];
@@ -347,15 +603,20 @@ __global__ void k_cand_slots(BatchDev b) {
     const InstPlan ip = b.insts[inst];
     const DictPlan dp = b.dicts[ip.dict];
     unsigned long long root = 0;
+    unsigned lmax = 0;
     for (int c = threadIdx.x; c < dp.chunks; c += blockDim.x) {
         const unsigned long long v = b.chunks[ip.chunk_off + c];
         root = v > root ? v : root;
+        lmax = max(lmax, b.chunk_l[ip.chunk_off + c]);
     }
     root = block_max_u64(root, red);  // valid in thread 0
+    // the largest certified lower bound of any slot: a lower bound of the best
+    const unsigned long long lkey = block_max_u64((unsigned long long)lmax, red);
     if (threadIdx.x == 0) {
         st.best32 = root;
         st.nbins = 0;
         s_root = root;
+        s_tstar = (unsigned)lkey;
     }
     __syncthreads();
     if ((unsigned)(s_root >> 32) == 0u) {  // nothing beats 0: src/gabor.cpp:108-110
@@ -365,12 +626,8 @@ __global__ void k_cand_slots(BatchDev b) {
         }
         return;
     }
-    const long long rs = (long long)(s_root & 0xffffffffull);
-    if (EMPI_BAD(rs >= dp.slots, 1)) return;
-    const float lroot = __uint_as_float((unsigned)(b.slots[ip.slot_off + rs] & 0xffffffffull));
+    const float lroot = __uint_as_float(s_tstar);
     const unsigned tbits = __float_as_uint(lroot * (1.0f - b.band));
-    if (threadIdx.x == 0) s_tstar = __float_as_uint(lroot);
-    __syncthreads();
     const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     for (int c = threadIdx.x >> 5; c < dp.chunks; c += nwarps) {
         if ((unsigned)(b.chunks[ip.chunk_off + c] >> 32) < tbits) continue;
@@ -622,6 +879,11 @@ __global__ void k_select(BatchDev b) {
         p[5] = phase;
     }
     if (threadIdx.x == 0) {
+        if (b.prange && it >= 1) {
+            // block proposal: did the atom lie in a proposed block?
+            atomicAdd(b.ctr + CTR_PROP_ITERS, 1);
+            if (in_range(b.prange[ip.ij_off + cb.j], cb.t)) atomicAdd(b.ctr + CTR_PROP_HITS, 1);
+        }
         b.indices[(long long)inst * b.iter_max + it] = make_int4(cb.j, cb.t, cb.k, nbins);
         st.it = it + 1;
         if (st.it >= b.iter_max) st.status = ST_DONE;  // src/classes.cpp:57-59

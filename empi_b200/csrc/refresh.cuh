@@ -997,6 +997,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
             if (!(U <= 3.0e38f)) U = 3.0e38f;  // NaN / inf inputs: keep the slot competitive
             out[(long long)(t_start + w) * sp.G + g] =
                 ((unsigned long long)__float_as_uint(U) << 32) | (unsigned long long)__float_as_uint(Lo);
+            if (b.stale) b.stale[ip.slot_off + sp.slot_base + (long long)(t_start + w) * sp.G + g] = 0;
         }
     }
     __syncthreads();

@@ -243,9 +243,65 @@ typedef struct {
     int wide_mask;            /* sub-FFT sizes (bit log2 L) with one 128-register CTA per SM, */
     int tuned;                /* and whether it came from the tune cache */
     int sizes_mask;           /* sub-FFT sizes (bit log2 L) the batch's dictionaries use */
+    /* proposal-ceiling probe (empi_batch_probe_proposal), summed over the run:
+     * slots the refresh rule recomputed, and those of them whose upper bound,
+     * propagated through the subtraction without recomputing, still reached
+     * the next certified best value (no exact proposal could skip them), with
+     * their reference-equivalent FFT work */
+    long long probe_dirty_slots, probe_needed_slots;
+    double probe_dirty_work, probe_needed_work;
+    /* block proposal (empi_batch_set_proposal): iterations that used one, and
+     * how many of their atoms lay in a proposed block (the hit rate) */
+    int proposal_iterations, proposal_hits;
 } empi_batch_stats;
 
 empi_status empi_batch_get_stats(empi_batch* batch, empi_batch_stats* stats);
+
+/* Enables (nonzero) or disables the proposal-ceiling probe of later runs (no
+ * counterpart in the reference).  A block proposal can skip a window's
+ * refresh only where a certified bound excludes it; the probe measures, on
+ * the plain decomposition, the share of the refresh rule's work (reference
+ * src/gabor.cpp:189-209) that no such proposal could skip.  Costs one float
+ * per slot and two extra kernels per iteration; the atoms are unchanged. */
+empi_status empi_batch_probe_proposal(empi_batch* batch, int enable);
+
+/* Block proposal for later runs (no counterpart in the reference; it changes
+ * how much of the refresh rule's work, src/gabor.cpp:189-209, is done, never
+ * the atoms).  After each subtraction a proposer scores 16 scale bands x 32
+ * time tiles; the dirty windows in the top k blocks are refreshed first, the
+ * other dirty windows get certified upper bounds propagated through the
+ * subtraction, and a second round refreshes those whose bound still reaches
+ * the best certified lower bound.  source: 0 the learned network (weights:
+ * a file written by empi_b200/proposal.py), 1 the blocks nearest the last
+ * atom, 2 none (k ignored: only the certified second round), -1 off.  The
+ * batch statistics report the hit rate.  Not for MMP1 (its constrained
+ * energy is not a norm of the window values). */
+empi_status empi_batch_set_proposal(empi_batch* batch, int source, int k, const char* weights);
+
+/* Training data for the learned proposal (no counterpart in the reference):
+ * with collection enabled, later runs keep the normalised 64 x 128
+ * log-spectrogram of every MP loop's residual before each selection;
+ * empi_batch_pairs then returns up to cap (spectrogram, block of the atom
+ * that selection chose) pairs -- spec: cap x 8192 floats, block: cap ints
+ * (band * 32 + tile) -- and their total in count. */
+empi_status empi_batch_collect_pairs(empi_batch* batch, int enable);
+empi_status empi_batch_pairs(empi_batch* batch, int cap, float* spec, int* block, int* count);
+
+/* The proposal network on a GPU, host arrays in and out (no counterpart in
+ * the reference).  Weights: empi_proposal_parameter_count() floats in the
+ * order of empi_b200/csrc/proposal.hpp.  scores: n x 512 block scores of n
+ * spectrograms, with BF16 tensor cores (bf16 = 1) or in FP32.  gradients:
+ * FP32 forward and backward of the mean softmax cross-entropy over n
+ * (spectrogram, block) pairs.  train: SGD with momentum, `epochs` shuffled
+ * passes in minibatches of `batch`, weights updated in place, each epoch's
+ * mean loss in losses (optional). */
+int empi_proposal_parameter_count(void);
+empi_status empi_proposal_scores(int device, const float* spec, int n, const float* weights, int bf16,
+                                 float* scores);
+empi_status empi_proposal_gradients(int device, const float* spec, const int* labels, int n,
+                                    const float* weights, float* grads, float* loss);
+empi_status empi_proposal_train(int device, const float* spec, const int* labels, int n, int epochs, int batch,
+                                float lr, float momentum, unsigned seed, float* weights, float* losses);
 
 /* One-shot convenience: create + load + run; atoms of epoch e go to
  * atoms + e * channels_e * cap * 6 in order (counts likewise per channel). */

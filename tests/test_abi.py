@@ -156,3 +156,22 @@ def test_tune_workload_key():
     assert autotune.workload_key("mmp3", w.epochs, w.fs, 0.01)["mode"] == 3
     u = synth.workload(3, epochs=3)
     assert autotune.workload_key("smp", u.epochs, u.fs, 0.01)["samples"] == 0
+
+
+def test_proposal_weights_format(tmp_path):
+    """The proposer's weights file: "EMPIPN01", int32 count, float32 parameters
+    in the layout the engine reads (empi_proposal_parameter_count)."""
+    from empi_b200 import proposal as P
+
+    assert P.parameter_count() == sum(int(np.prod(s)) for _, s in P.LAYOUT) == 22256
+    w = P.init_weights(4)
+    path = tmp_path / "w.bin"
+    P.save_weights(str(path), w)
+    data = path.read_bytes()
+    assert data[:8] == b"EMPIPN01" and len(data) == 12 + 4 * w.size
+    np.testing.assert_array_equal(P.load_weights(str(path)), w)
+    path.write_bytes(b"EMPIPN00" + data[8:])
+    with pytest.raises(ValueError):
+        P.load_weights(str(path))
+    parts = P.unpack(w)
+    assert parts["w2"].shape == (32, 16, 3, 3) and parts["b4"].shape == (16,)

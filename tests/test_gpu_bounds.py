@@ -157,3 +157,27 @@ def test_candidate_flood_gives_the_same_atoms(engine, name):
     np.testing.assert_array_equal(got.indices, ref.indices[..., :3] if got.indices.shape != ref.indices.shape
                                   else ref.indices)
     np.testing.assert_allclose(got.atoms, ref.atoms, rtol=1e-12, atol=1e-300)
+
+
+def test_proposal_probe_leaves_atoms_unchanged(engine):
+    """The proposal-ceiling probe (empi_batch_probe_proposal) only measures:
+    same atoms, and the refresh work no certified proposal could skip is part
+    of the work the refresh rule did."""
+    from empi_b200 import synth
+
+    w = synth.workload(1, epochs=2, channels=4, samples=2000, seed=9)
+    settings = empi_b200.DecompositionSettings(20, 1.0 - 0.01 * w.energy_percent)
+    ref = empi_b200.decompose_epochs("mmp2", w.epochs, w.fs, w.energy_error, 20, w.energy_percent, engine=engine)
+    b = empi_b200.Batch("mmp2", w.energy_error, settings, [e.shape for e in w.epochs], w.fs, engine=engine)
+    b.probe_proposal(True)
+    b.load(w.epochs)
+    b.run()
+    st = b.stats()
+    got = [b.result(e) for e in range(2)]
+    b.close()
+    for g, r in zip(got, ref):
+        np.testing.assert_array_equal(g.indices, r.indices)
+        np.testing.assert_allclose(g.atoms, r.atoms, rtol=1e-12, atol=0)
+    assert st.probe_dirty_slots > 0 and 0 <= st.probe_needed_slots <= st.probe_dirty_slots
+    assert 0 < st.probe_needed_work <= st.probe_dirty_work
+    print(f"needed {st.probe_needed_work / st.probe_dirty_work:.3f} of the refresh work")

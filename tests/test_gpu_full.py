@@ -2,10 +2,16 @@
 
 The fixtures under tests/golden/full/ were generated by
 tests/golden/make_golden.py --full from the reference's own decomposition
-classes (empi's src/*.cpp built by oracle/Makefile).
+classes (empi's src/*.cpp built by oracle/Makefile), except the energyError
+0.001 case, whose reference workspace (~108 GB) does not fit the generating
+host: that one is pinned to the restatement (oracle/mp_oracle.c), itself
+pinned to the reference on every smaller golden.
 
   mmp2_19x8x5120        every atom of the 8-epoch MMP2 bench workload
   mmp3_4x16384_512      MMP3 at 16384 samples @ 512 Hz, 4 channels, 50 atoms
+  smp_batch_16x2        16 of the 512 batched SMP instances (two channels each),
+                        150 iterations, decomposed in one uneven batch
+  smp_16384_512_eps0001 energyError 0.001, Nfft up to 2^20 (144 scales)
 
 Each test reports how many atoms it compared; the parity rule is
 helpers.compare_sequences' (at least 95 % compared, indices exact outside
@@ -64,9 +70,11 @@ def run_and_compare(engine, name):
             e_got = r.energies[c] if smp else r.energies
             # residual energies belong to the MP loop: per channel for SMP, once otherwise
             check_e = smp or c == 0
+            # the 95 % rule is asserted over the test's atoms below: a genuine
+            # near-tie in one channel exempts the rest of that channel only
             n = compare_sequences(g["atoms"][c, :n_ref], r.atoms[c, : r.counts[c]], g["margins"][l],
                                   g["energies"][l] if check_e else None, e_got if check_e else None,
-                                  label=f"{name} epoch {e} ch{c}")
+                                  label=f"{name} epoch {e} ch{c}", min_fraction=0.0)
             if c < loops:  # an MMP atom counts once, an SMP channel is its own loop
                 compared += n
                 total += n_ref
@@ -82,3 +90,11 @@ def test_mmp2_19x8x5120_every_atom(engine):
 
 def test_mmp3_4x16384_512(engine):
     run_and_compare(engine, "mmp3_4x16384_512")
+
+
+def test_smp_batch_16_instances(engine):
+    run_and_compare(engine, "smp_batch_16x2")
+
+
+def test_energy_error_0001_nfft_2_20_against_restatement(engine):
+    run_and_compare(engine, "smp_16384_512_eps0001")

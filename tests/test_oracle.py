@@ -92,7 +92,7 @@ def test_subtract_fit_matches_reference_values():
     assert abs(p[1] - mod / nrm) < 1e-12 * abs(mod / nrm)
 
 
-FULL_FIXTURES = ["mmp2_19x8x5120", "mmp3_4x16384_512"]
+FULL_FIXTURES = ["mmp2_19x8x5120", "mmp3_4x16384_512", "smp_batch_16x2", "smp_16384_512_eps0001"]
 
 
 @pytest.mark.parametrize("name", FULL_FIXTURES)
