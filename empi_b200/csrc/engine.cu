@@ -346,6 +346,7 @@ struct empi_batch {
     empi_batch_stats stats{};
     int launches_per_iter = 10;
     int regrows = 0;  // candidate-buffer growths (overflow recoveries) so far
+    int total_chunks = 0;  // leaf chunks of all instances
 
     ~empi_batch() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -470,7 +471,7 @@ void launch_proposal_update(empi_batch* b, cudaStream_t s, cudaEvent_t e0, cudaE
     k_propagate_stale<<<b->tree_grid, 256, 0, s>>>(b->dev);
     k_tree<<<b->tree_grid, 256, 0, s>>>(b->dev);
     k_root<<<ninst, 256, 0, s>>>(b->dev);
-    k_qualify<<<ninst, 256, 0, s>>>(b->dev);
+    k_qualify<<<b->tree_grid, 256, 0, s>>>(b->dev, b->total_chunks);
     cudaMemsetAsync(b->dev.lcount, 0, sizeof(int) * 2 * 16, s);
     k_round2_sched<<<ninst, 128, 0, s>>>(b->dev);
     launch_refresh(b, s);
@@ -647,6 +648,7 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
     CUDA_TRY(b->d_state.alloc(ninst));
     CUDA_TRY(b->d_slots.alloc(slot_off));
     CUDA_TRY(b->d_chunks.alloc(chunk_off));
+    b->total_chunks = (int)chunk_off;
     CUDA_TRY(b->d_chunk_l.alloc(chunk_off));
     CUDA_TRY(b->d_dirty.alloc(ij_off));
     CUDA_TRY(b->d_crange.alloc(ij_off));

@@ -526,20 +526,30 @@ __global__ void k_root(BatchDev b) {
     if (threadIdx.x == 0) st.lround = (unsigned)l;
 }
 
-// per instance: every stale slot (propagated bounds, in this iteration's
-// dirty set or left from earlier ones) whose upper bound reaches the largest
-// certified lower bound; the tree's chunk maxima skip the chunks below it.
-// Qualifying windows widen their scale's round-2 range.
-__global__ void k_qualify(BatchDev b) {
-    const int inst = blockIdx.x;
-    const InstState& st = b.state[inst];
-    if (st.status != ST_RUNNING || st.it < 1) return;
-    const InstPlan ip = b.insts[inst];
-    const DictPlan dp = b.dicts[ip.dict];
-    const unsigned lb = st.lround;
-    const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    for (int c = threadIdx.x >> 5; c < dp.chunks; c += nwarps) {
-        if ((unsigned)(b.chunks[ip.chunk_off + c] >> 32) < lb) continue;
+// Every stale slot (propagated bounds, from this iteration's dirty set or left
+// from earlier ones) whose upper bound reaches its instance's largest
+// certified lower bound: a warp per leaf chunk over all instances' chunks,
+// skipping chunks whose maximum is below it.  Qualifying windows widen their
+// scale's round-2 range.
+__global__ void k_qualify(BatchDev b, int total_chunks) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int item = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); item < total_chunks; item += nwarps) {
+        // the instance owning global chunk `item` (chunk_off is a prefix over instances)
+        int lo = 0, hi = b.ninst - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (b.insts[mid].chunk_off <= item) lo = mid;
+            else hi = mid - 1;
+        }
+        const int inst = lo;
+        const InstState& st = b.state[inst];
+        if (st.status != ST_RUNNING || st.it < 1) continue;
+        const InstPlan ip = b.insts[inst];
+        const unsigned lb = st.lround;
+        const int c = item - (int)ip.chunk_off;
+        if ((unsigned)(b.chunks[item] >> 32) < lb) continue;
+        const DictPlan dp = b.dicts[ip.dict];
         const long long s0 = (long long)c * kChunk;
         const long long s1 = min(s0 + kChunk, dp.slots);
         for (long long s = s0 + lane; s < s1; s += 32) {
