@@ -53,6 +53,9 @@ def parse():
                    help="weak: every rank decomposes its own copy of the workload (the default); strong: one "
                         "workload split across the ranks by estimated cost (empi_b200.shard)")
     p.add_argument("--no-roofline", action="store_true")
+    p.add_argument("--persistent", type=int, default=-1, choices=[-1, 0, 1],
+                   help="the MP loop as one persistent kernel per chunk (1), as the CUDA graph (0), or by the "
+                        "tune cache / batch size (-1, the default)")
     p.add_argument("--proposal", choices=["net", "last_atom", "none"],
                    help="time the block proposal too (same workload, plain and proposal back to back; the atoms "
                         "must be identical); net uses --proposal-weights")
@@ -283,7 +286,8 @@ def ours(args):
 
     # the committed autotuner cache: launch shapes tuned on a B200 per workload
     tune_cache = autotune.DEFAULT_CACHE if os.path.exists(autotune.DEFAULT_CACHE) else None
-    eng = empi_b200.Engine(device=local, stream=stream.cuda_stream, tune_cache=tune_cache)
+    eng = empi_b200.Engine(device=local, stream=stream.cuda_stream, tune_cache=tune_cache,
+                           persistent=args.persistent)
     settings = empi_b200.DecompositionSettings(w.iterations, 1.0 - 0.01 * w.energy_percent)
     shapes = [e.shape for e in w.epochs]
     pinned = [torch.from_numpy(e).pin_memory() for e in w.epochs]
@@ -455,7 +459,8 @@ def ours(args):
             "candidate_bins_per_atom": bs.candidate_bins / max(1, bs.atoms),
             "proposal_ceiling": ceiling, "proposal": proposal,
             "launch_shape": {"transform_cap": bs.transform_cap, "iterations_per_graph": bs.iterations_per_graph,
-                             "wide_mask": bs.wide_mask, "tuned": bool(bs.tuned)},
+                             "wide_mask": bs.wide_mask, "tuned": bool(bs.tuned),
+                             "persistent": bool(bs.persistent)},
         }
         print(json.dumps(line))
     batch.close()

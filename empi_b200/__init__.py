@@ -42,7 +42,8 @@ _VARIANTS = {"smp": SMP, "mmp1": MMP1, "mmp2": MMP2, "mmp3": MMP3}
 class EngineOpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("stream", ctypes.c_void_p), ("transform_cap", ctypes.c_int),
                 ("candidate_band", ctypes.c_double), ("candidate_capacity", ctypes.c_int),
-                ("iterations_per_graph", ctypes.c_int), ("timing", ctypes.c_int), ("tune_cache", ctypes.c_char_p)]
+                ("iterations_per_graph", ctypes.c_int), ("timing", ctypes.c_int), ("tune_cache", ctypes.c_char_p),
+                ("persistent", ctypes.c_int), ("wait_limit_ms", ctypes.c_int), ("test_unreachable_wait", ctypes.c_int)]
 
 
 class Dictionary(ctypes.Structure):
@@ -69,7 +70,7 @@ class BatchStats(ctypes.Structure):
                 ("sizes_mask", ctypes.c_int), ("probe_dirty_slots", ctypes.c_longlong),
                 ("probe_needed_slots", ctypes.c_longlong), ("probe_dirty_work", ctypes.c_double),
                 ("probe_needed_work", ctypes.c_double), ("proposal_iterations", ctypes.c_int),
-                ("proposal_hits", ctypes.c_int)]
+                ("proposal_hits", ctypes.c_int), ("persistent", ctypes.c_int)]
 
 
 EXPORTS = [
@@ -82,7 +83,7 @@ EXPORTS = [
     "empi_decompose", "empi_run_config", "empi_book_write", "empi_subtract_atom_from_signal_noalloc",
     "empi_dictionary_error_bounds", "empi_tune_lookup", "empi_batch_probe_proposal", "empi_batch_set_proposal",
     "empi_batch_collect_pairs", "empi_batch_pairs", "empi_proposal_parameter_count", "empi_proposal_scores",
-    "empi_proposal_gradients", "empi_proposal_train",
+    "empi_proposal_gradients", "empi_proposal_train", "empi_batch_tree",
 ]
 
 _lib = None
@@ -113,7 +114,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.empi_dictionary_error_bounds.argtypes = [ctypes.POINTER(Dictionary), ctypes.c_double, ctypes.c_int,
                                                ctypes.c_int, fp, fp, fp, ip, ip, ip]
     L.empi_tune_lookup.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
-                                   ctypes.c_double, ip, ip, ip]
+                                   ctypes.c_double, ip, ip, ip, ip]
     L.empi_workspace_create.argtypes = [vp, ctypes.POINTER(Dictionary), ctypes.c_double, ctypes.c_int,
                                         ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
     L.empi_workspace_destroy.argtypes = [vp]
@@ -139,6 +140,9 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     L.empi_batch_set_proposal.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_char_p]
     L.empi_batch_collect_pairs.argtypes = [vp, ctypes.c_int]
     L.empi_batch_pairs.argtypes = [vp, ctypes.c_int, fp, ip, ip]
+    u64p = ctypes.POINTER(ctypes.c_uint64)
+    L.empi_batch_tree.argtypes = [vp, ctypes.c_int, ctypes.c_longlong, u64p, ctypes.POINTER(ctypes.c_longlong),
+                                  ctypes.c_int, u64p, ctypes.POINTER(ctypes.c_uint32), ip]
     L.empi_proposal_parameter_count.restype = ctypes.c_int
     L.empi_proposal_scores.argtypes = [ctypes.c_int, fp, ctypes.c_int, fp, ctypes.c_int, fp]
     L.empi_proposal_gradients.argtypes = [ctypes.c_int, fp, ip, ctypes.c_int, fp, fp, fp]
@@ -185,7 +189,8 @@ class Engine:
 
     def __init__(self, device: int = 0, stream: int | None = None, transform_cap: int = 0,
                  candidate_band: float = 0.0, candidate_capacity: int = 0, iterations_per_graph: int = 0,
-                 timing: bool = False, tune_cache: str | None = None):
+                 timing: bool = False, tune_cache: str | None = None, persistent: int = -1,
+                 wait_limit_ms: int = 0, test_unreachable_wait: bool = False):
         L = load_library()
         o = EngineOpts()
         L.empi_engine_opts_default(ctypes.byref(o))
@@ -201,6 +206,10 @@ class Engine:
             o.iterations_per_graph = iterations_per_graph
         o.timing = int(timing)
         o.tune_cache = os.fsencode(tune_cache) if tune_cache else None
+        o.persistent = int(persistent)
+        if wait_limit_ms:
+            o.wait_limit_ms = int(wait_limit_ms)
+        o.test_unreachable_wait = int(bool(test_unreachable_wait))
         h = ctypes.c_void_p()
         _check(L.empi_engine_create(ctypes.byref(o), ctypes.byref(h)))
         self.handle = h
@@ -301,18 +310,20 @@ def dictionary_error_bounds(energyError, freqSampling, sampleCount, scaleMin=0.0
 
 
 def tune_lookup(path, mode, channels, fs, samples, energy_error):
-    """(transform_cap, iterations_per_graph, wide_mask) of the tune cache's
-    entry for a workload, or None (empi_tune_lookup; no GPU needed)."""
+    """(transform_cap, iterations_per_graph, wide_mask, persistent) of the tune
+    cache's entry for a workload (persistent -1: not tuned), or None
+    (empi_tune_lookup; no GPU needed)."""
     L = load_library()
-    cap, k, wide = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    cap, k, wide, pers = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
     st = L.empi_tune_lookup(os.fsencode(path), int(mode), int(channels), float(fs), int(samples),
-                            float(energy_error), ctypes.byref(cap), ctypes.byref(k), ctypes.byref(wide))
+                            float(energy_error), ctypes.byref(cap), ctypes.byref(k), ctypes.byref(wide),
+                            ctypes.byref(pers))
     if st != 0:
         msg = (L.empi_last_error() or b"").decode()
         if msg == "noTunedEntry":
             return None
         raise EmpiError(st, msg)
-    return cap.value, k.value, wide.value
+    return cap.value, k.value, wide.value, pers.value
 
 
 # ---------------------------------------------------------------- workspace seam
@@ -485,6 +496,22 @@ class Batch:
             _check(L.empi_batch_pairs(self.handle, n.value, spec.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
                                       _ip(blocks), ctypes.byref(n)))
         return spec, blocks
+
+    def tree(self, instance):
+        """(slot keys [S] uint64, leaf-chunk maxima [K] uint64, chunk lower
+        bounds [K] uint32) of MP loop `instance` (empi_batch_tree)."""
+        L = load_library()
+        ns, nc = ctypes.c_longlong(), ctypes.c_int()
+        _check(L.empi_batch_tree(self.handle, int(instance), 0, None, ctypes.byref(ns), 0, None, None,
+                                 ctypes.byref(nc)))
+        slots = np.zeros(ns.value, np.uint64)
+        chunks = np.zeros(nc.value, np.uint64)
+        chunk_l = np.zeros(nc.value, np.uint32)
+        u64p = ctypes.POINTER(ctypes.c_uint64)
+        _check(L.empi_batch_tree(self.handle, int(instance), ns.value, slots.ctypes.data_as(u64p), ctypes.byref(ns),
+                                 nc.value, chunks.ctypes.data_as(u64p),
+                                 chunk_l.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), ctypes.byref(nc)))
+        return slots, chunks, chunk_l
 
     def probe_proposal(self, enable=True):
         """Measure, in later runs, the refresh work no certified block

@@ -15,7 +15,10 @@ whole batch runs (CUDA events, stats.run_ms), over:
 * iterations_per_graph -- MP iterations per CUDA-graph launch (4, 8, 16);
 * per sub-FFT size present in the workload, the refresh variant: two CTAs per
   SM at 64 registers (the default) or one at 128 registers without spills
-  (wide_mask bit log2 L).
+  (wide_mask bit log2 L);
+* persistent -- the MP loop as one persistent cooperative kernel per chunk of
+  iterations (1) or as the multi-kernel CUDA graph (0); the engine's own
+  choice, without a tuned entry, is by batch size.
 
 The search is coordinate descent from the default shape, keeping a change only
 when it is faster by more than 1 %, and every candidate shape is checked to
@@ -99,6 +102,7 @@ class _Trial:
             times.append(b.stats().run_ms)
         st = b.stats()
         assert st.tuned == 1 and st.transform_cap == shape["transform_cap"]
+        assert "persistent" not in shape or st.persistent == shape["persistent"]
         atoms = [b.result(e) for e in range(len(self.epochs))]
         b.close()
         eng.close()
@@ -135,6 +139,9 @@ def tune(variant, epochs, fs, energy_error, iterations, energy_percent, device=0
         consider(dict(best, transform_cap=cap))
     for k in GRAPH_ITERS[1:]:
         consider(dict(best, iterations_per_graph=k))
+    # the loop's form: graph or persistent kernel, against the engine's default
+    # by batch size (what the default shape above ran)
+    consider(dict(best, persistent=0 if st0.persistent else 1))
     # the sizes present depend on the cap: read them from a run with the best one
     _, st, _ = trial.run(best, 1)
     for lg in range(13):

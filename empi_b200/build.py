@@ -24,14 +24,14 @@ BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
                      "--expt-relaxed-constexpr", "-diag-suppress", "177"]
-SOURCES = ["engine.cu", "refresh_single.cu", "refresh_mmp1.cu", "refresh_mmp3.cu", "proposal.cu", "geometry.cpp",
-           "hostio.cpp", "tune.cpp"]
+SOURCES = ["engine.cu", "refresh_single.cu", "refresh_mmp1.cu", "refresh_mmp3.cu", "persist_single.cu",
+           "persist_mmp1.cu", "persist_mmp3.cu", "proposal.cu", "geometry.cpp", "hostio.cpp", "tune.cpp"]
 # Device code of the engine: single-precision math with approximate division,
 # square root and exp2 and flush-to-zero (the FP32 energy maps; FP64 code is
 # unaffected).  The FP32 maps only rank candidates: every bin within 1e-4 of
 # the maximum is re-scored in FP64, and the parity tests bound the map error.
 ENGINE_FLAGS = ["--use_fast_math"]
-HEADERS = ["fft.cuh", "common.cuh", "kernels.cuh", "refresh.cuh", "refresh_kernels.hpp", "plan.hpp", "geometry.hpp",
+HEADERS = ["fft.cuh", "common.cuh", "kernels.cuh", "refresh.cuh", "persist.cuh", "refresh_kernels.hpp", "plan.hpp", "geometry.hpp",
            "engine.hpp", "tune.hpp", "proposal.hpp"]
 
 

@@ -82,6 +82,15 @@ struct CandBin {
     double e64;
 };
 
+// Grid barrier of the persistent kernel: arrivals of the current generation,
+// the generation, and the error record (0, or 1 + the phase whose wait ran out).
+struct GridSync {
+    unsigned count;
+    unsigned gen;
+    int err;
+    int pad_;
+};
+
 struct BatchDev {
     const ScalePlan* scales;
     const DictPlan* dicts;
@@ -140,9 +149,38 @@ struct BatchDev {
     int2* qrange;
     int prop_k;
     unsigned char* stale;  // block proposal: per slot, 1 while its key holds propagated bounds
+    // persistent kernel (persist.cuh): its grid barrier, the time limit of a
+    // wait in nanoseconds, and extra arrivals a barrier waits for (0; 1 only
+    // in the test that makes every wait run out)
+    GridSync* gsync;
+    long long wait_ns;
+    int wait_extra;
 };
 
+
 // ------------------------------------------------------------ helpers
+
+// Loads of data that a persistent launch rewrites between its iterations (the
+// FP32 residual, the refresh unit lists, the schedule's prefix sums).  Across
+// separate kernels they take the read-only path (__ldg, __restrict__); inside
+// the persistent kernel (translation units defining EMPI_PHASES_ONLY) they
+// must be ordinary loads, which the grid barrier's fences order -- the
+// read-only path is outside the memory model and could return a line another
+// SM has rewritten since.
+#ifdef EMPI_PHASES_ONLY
+#define EMPI_RESTRICT_MUT
+template <class T>
+__device__ __forceinline__ T ld_mut(const T* p) {
+    return *p;
+}
+#else
+#define EMPI_RESTRICT_MUT __restrict__
+template <class T>
+__device__ __forceinline__ T ld_mut(const T* p) {
+    return __ldg(p);
+}
+#endif
+
 
 __device__ __forceinline__ unsigned long long pack_key(float e, unsigned low) {
     if (!(e >= 0.0f && e <= 3.0e38f)) e = 0.0f;
@@ -199,7 +237,7 @@ __device__ __forceinline__ int upper_index(const int* prefix, int n, int u) {
     int lo = 0, hi = n - 1;
     while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;
-        if (__ldg(prefix + mid) <= u) lo = mid;
+        if (ld_mut(prefix + mid) <= u) lo = mid;
         else hi = mid - 1;
     }
     return lo;

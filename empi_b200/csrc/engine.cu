@@ -70,6 +70,7 @@ extern "C" const char* empi_status_string(empi_status st) {
         case EMPI_ERR_IO: return "ioError";
         case EMPI_ERR_NO_DEVICE: return "noCudaDevice";
         case EMPI_ERR_INTERNAL: return "internalError";
+        case EMPI_ERR_DEVICE_WAIT_TIMEOUT: return "deviceWaitTimeout";
     }
     return "unknown";
 }
@@ -77,6 +78,7 @@ extern "C" const char* empi_status_string(empi_status st) {
 // ------------------------------------------------------------ engine
 
 constexpr int kSizes = kRefreshSizes;  // sub-FFT sizes 2^0 .. 2^12, one refresh kernel each
+constexpr long long kPersistAutoSlots = 1LL << 19;  // batches up to this many slot keys run persistent
 
 struct empi_engine {
     empi_engine_opts opts;
@@ -98,6 +100,8 @@ extern "C" void empi_engine_opts_default(empi_engine_opts* o) {
     o->candidate_band = 0.0;
     o->candidate_capacity = 0;
     o->iterations_per_graph = 8;
+    o->persistent = -1;
+    o->wait_limit_ms = 1000;
 }
 
 namespace {
@@ -119,6 +123,8 @@ extern "C" empi_status empi_engine_create(const empi_engine_opts* opts, empi_eng
         if (e->opts.transform_cap == 0) e->opts.transform_cap = 4096;
         if (!(e->opts.candidate_band >= 0.0) || e->opts.candidate_band >= 1.0) e->opts.candidate_band = 0.0;
         if (e->opts.iterations_per_graph <= 0) e->opts.iterations_per_graph = 8;
+        if (e->opts.persistent < -1 || e->opts.persistent > 1) e->opts.persistent = -1;
+        if (e->opts.wait_limit_ms <= 0) e->opts.wait_limit_ms = 1000;
     }
     int n = 0;
     cudaError_t ce = cudaGetDeviceCount(&n);
@@ -150,6 +156,9 @@ extern "C" empi_status empi_engine_create(const empi_engine_opts* opts, empi_eng
     refresh_kernels_single(e->rk[0]);
     refresh_kernels_mmp1(e->rk[1]);
     refresh_kernels_mmp3(e->rk[2]);
+    persist_kernel_single(e->rk[0]);
+    persist_kernel_mmp1(e->rk[1]);
+    persist_kernel_mmp3(e->rk[2]);
     if (e->opts.tune_cache) e->tune_cache = e->opts.tune_cache;
     e->opts.tune_cache = nullptr;  // the engine keeps its own copy
     CUDA_TRY(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
@@ -237,7 +246,7 @@ extern "C" empi_status empi_dictionary_error_bounds(const empi_dictionary* d, do
 
 extern "C" empi_status empi_tune_lookup(const char* path, int mode, int channels, double fs, int samples,
                                         double energy_error, int* transform_cap, int* iterations_per_graph,
-                                        int* wide_mask) {
+                                        int* wide_mask, int* persistent) {
     if (!path) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
     TuneParams tp;
     std::string err;
@@ -246,6 +255,7 @@ extern "C" empi_status empi_tune_lookup(const char* path, int mode, int channels
     if (transform_cap) *transform_cap = tp.transform_cap;
     if (iterations_per_graph) *iterations_per_graph = tp.iterations_per_graph;
     if (wide_mask) *wide_mask = tp.wide_mask;
+    if (persistent) *persistent = tp.persistent;
     return ok();
 }
 
@@ -334,6 +344,12 @@ struct empi_batch {
     // one-CTA-per-SM refresh variants, and whether the tune cache set them
     int lcap = 4096, K = 8, wide_mask = 0;
     bool tuned = false;
+    // the persistent kernel (persist.cuh): the tune cache's choice (-1: none),
+    // whether this batch runs it, its grid and its barrier
+    int tuned_persistent = -1;
+    bool persistent = false;
+    int persist_grid = 0;
+    DevBuf<GridSync> d_gsync;
     size_t refresh_smem = 0;             // the candidate kernel's (largest layout)
     size_t refresh_smem_lg[kSizes] = {};  // per sub-FFT size
 
@@ -347,6 +363,7 @@ struct empi_batch {
     int launches_per_iter = 10;
     int regrows = 0;  // candidate-buffer growths (overflow recoveries) so far
     int total_chunks = 0;  // leaf chunks of all instances
+    long long total_slots = 0;  // slot keys of all instances
 
     ~empi_batch() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -392,6 +409,29 @@ empi_status configure(empi_batch* b) {
     CUDA_TRY(cudaFuncSetAttribute(b->collect_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk.collect_smem));
     b->refresh_smem = rk.collect_smem;
     b->collect_grid = b->eng->sms;
+    // The persistent kernel: the engine's option, else the tune cache's
+    // choice, else small batches only (below kPersistAutoSlots slot keys the
+    // per-iteration work is a few microseconds per step and the graph is bound
+    // by launch latency; above it the graph's two-CTAs-per-SM refresh is
+    // faster).  It needs one co-resident 512-thread CTA per SM.
+    int want = b->eng->opts.persistent;
+    if (want < 0) want = b->tuned_persistent;
+    if (want < 0) want = (long long)b->total_slots <= kPersistAutoSlots ? 1 : 0;
+    b->persistent = false;
+    int coop = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, b->eng->device));
+    if (want == 1 && coop && rk.persist) {
+        int o = 0;
+        CUDA_TRY(cudaFuncSetAttribute(rk.persist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk.persist_smem));
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, rk.persist, kUnitThreads, rk.persist_smem) ==
+                cudaSuccess &&
+            o >= 1) {
+            b->persistent = true;
+            b->persist_grid = b->eng->sms;
+            CUDA_TRY(b->d_gsync.alloc(1));
+        }
+        cudaGetLastError();  // a layout that does not fit is not an error: the graph runs
+    }
     return EMPI_OK;
 }
 
@@ -527,6 +567,7 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
                 b->lcap = tp.transform_cap;
             if (tp.iterations_per_graph > 0 && tp.iterations_per_graph <= 64) b->K = tp.iterations_per_graph;
             b->wide_mask = tp.wide_mask & ((1 << kSizes) - 1);
+            b->tuned_persistent = tp.persistent;
             b->tuned = true;
         } else if (terr != "noTunedEntry") {
             return fail(EMPI_ERR_CONFIG, terr);
@@ -649,6 +690,7 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
     CUDA_TRY(b->d_slots.alloc(slot_off));
     CUDA_TRY(b->d_chunks.alloc(chunk_off));
     b->total_chunks = (int)chunk_off;
+    b->total_slots = slot_off;
     CUDA_TRY(b->d_chunk_l.alloc(chunk_off));
     CUDA_TRY(b->d_dirty.alloc(ij_off));
     CUDA_TRY(b->d_crange.alloc(ij_off));
@@ -739,6 +781,9 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
     d.dump = nullptr;
     st = configure(b.get());
     if (st != EMPI_OK) return st;
+    d.gsync = b->d_gsync.p;
+    d.wait_ns = (long long)eng->opts.wait_limit_ms * 1000000LL;
+    d.wait_extra = eng->opts.test_unreachable_wait ? 1 : 0;
     b->tree_grid = eng->sms * 8;
     b->rescore_grid = eng->sms;
     if (b->max_n * sizeof(double) > 48 * 1024 && !b->fit_map.empty()) {
@@ -806,6 +851,13 @@ empi_status grow_candidates(empi_batch* b) {
     return EMPI_OK;
 }
 
+// The persistent kernel runs when the batch chose it and nothing needs the
+// multi-kernel form: per-kernel timing events, the block proposal, the probe
+// or the training-pair collection.
+bool runs_persistent(const empi_batch* b) {
+    return b->persistent && !b->eng->opts.timing && !b->dev.prop && !b->dev.prange && !b->collect;
+}
+
 empi_status capture_graph(empi_batch* b) {
     const int K = b->K;
     const bool timing = b->eng->opts.timing != 0;
@@ -814,6 +866,7 @@ empi_status capture_graph(empi_batch* b) {
         for (auto& e : b->ev) CUDA_TRY(cudaEventCreate(&e));
     }
     if (b->graph || timing) return EMPI_OK;  // timing mode launches eagerly, events between kernels
+    if (runs_persistent(b)) return EMPI_OK;
     cudaStream_t s = b->eng->stream;
     cudaGraph_t g = nullptr;
     CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -949,6 +1002,7 @@ empi_status batch_run_hooked(empi_batch* b, const std::function<void()>& after_c
     }
     const int imax = b->settings.iteration_max;
     const int K = b->K;
+    const bool persistent = runs_persistent(b);
     // every instance stops itself after imax atoms; a chunk in which some
     // instances stall on a candidate overflow costs at most one extra chunk
     const int max_regrows = 12;
@@ -958,14 +1012,28 @@ empi_status batch_run_hooked(empi_batch* b, const std::function<void()>& after_c
         if (timing) {
             for (int k = 0; k < K; ++k) launch_iteration(b, s, b->ev[2 * (k + 1)], b->ev[2 * (k + 1) + 1]);
             CUDA_TRY(cudaGetLastError());
+            launches += K * b->launches_per_iter;
+        } else if (persistent) {
+            // one cooperative launch per chunk: every CTA co-resident, or the
+            // launch fails (no barrier can wait on a CTA that never runs)
+            CUDA_TRY(cudaMemsetAsync(b->d_gsync.p, 0, sizeof(GridSync), s));
+            int iters = K;
+            void* args[] = {&b->dev, &iters};
+            const RefreshKernels& rk = kernels_of(b->eng, b->mode);
+            CUDA_TRY(cudaLaunchCooperativeKernel(rk.persist, dim3(b->persist_grid), dim3(kUnitThreads), args,
+                                                 rk.persist_smem, s));
+            launches += 1;
         } else {
             CUDA_TRY(cudaGraphLaunch(b->graph, s));
+            launches += K * b->launches_per_iter;
         }
         ++chunks;
-        launches += K * b->launches_per_iter;
         int ctr_now[CTR_COUNT];
+        GridSync gs{};
         CUDA_TRY(cudaMemcpyAsync(ctr_now, b->d_ctr.p, sizeof(ctr_now), cudaMemcpyDeviceToHost, s));
+        if (persistent) CUDA_TRY(cudaMemcpyAsync(&gs, b->d_gsync.p, sizeof(gs), cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaStreamSynchronize(s));
+        if (gs.err) return fail(EMPI_ERR_DEVICE_WAIT_TIMEOUT, "deviceWaitTimeout:phase" + std::to_string(gs.err - 1));
         if (timing) {
             for (int k = 0; k < K; ++k) {
                 float ms = 0.f;
@@ -1030,6 +1098,7 @@ empi_status batch_run_hooked(empi_batch* b, const std::function<void()>& after_c
     b->stats.tuned = b->tuned ? 1 : 0;
     b->stats.proposal_iterations = ctr[CTR_PROP_ITERS];
     b->stats.proposal_hits = ctr[CTR_PROP_HITS];
+    b->stats.persistent = persistent ? 1 : 0;
     if (b->dev.probe) {
         double pr[4];
         CUDA_TRY(cudaMemcpy(pr, b->dev.probe, sizeof(pr), cudaMemcpyDeviceToHost));
@@ -1126,6 +1195,32 @@ extern "C" empi_status empi_batch_pairs(empi_batch* b, int cap, float* spec, int
         }
     }
     *count = n;
+    return ok();
+}
+
+extern "C" empi_status empi_batch_tree(empi_batch* b, int instance, long long slot_cap, unsigned long long* slots,
+                                       long long* slot_count, int chunk_cap, unsigned long long* chunks,
+                                       unsigned* chunk_l, int* chunk_count) {
+    if (!b || !slot_count || !chunk_count || instance < 0 || instance >= (int)b->insts.size())
+        return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    const InstPlan& ip = b->insts[instance];
+    const DictPlan& dp = b->dicts[ip.dict];
+    *slot_count = dp.slots;
+    *chunk_count = dp.chunks;
+    if (!slots && !chunks && !chunk_l) return ok();
+    if ((slots && slot_cap < dp.slots) || ((chunks || chunk_l) && chunk_cap < dp.chunks))
+        return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
+    empi_status st = set_device(b->eng);
+    if (st != EMPI_OK) return st;
+    if (slots)
+        CUDA_TRY(cudaMemcpy(slots, b->d_slots.p + ip.slot_off, sizeof(unsigned long long) * dp.slots,
+                            cudaMemcpyDeviceToHost));
+    if (chunks)
+        CUDA_TRY(cudaMemcpy(chunks, b->d_chunks.p + ip.chunk_off, sizeof(unsigned long long) * dp.chunks,
+                            cudaMemcpyDeviceToHost));
+    if (chunk_l)
+        CUDA_TRY(cudaMemcpy(chunk_l, b->d_chunk_l.p + ip.chunk_off, sizeof(unsigned) * dp.chunks,
+                            cudaMemcpyDeviceToHost));
     return ok();
 }
 

@@ -11,10 +11,21 @@
 //   k_sched_a/b   stop test, dirty t-range per scale, work-unit prefix sums
 //   k_refresh     windowed FFT + energies + per-slot max over the dirty range
 //   k_tree        leaf-chunk maxima for the chunks the refresh touched
-// Waits are never spun on: ordering comes from kernel boundaries only.
+// In this multi-kernel form nothing spins: ordering comes from kernel
+// boundaries.  The same per-iteration steps run as phases of one persistent
+// kernel for small batches (persist.cuh), separated by a bounded grid barrier;
+// each kernel here is a thin wrapper around its phase body.
 #pragma once
 
 #include "common.cuh"
+
+// A translation unit that includes this file for the phase bodies only (the
+// persistent kernel's) gets its own internal copies of the wrapper kernels.
+#ifdef EMPI_PHASES_ONLY
+#define EMPI_GLOBAL static __global__
+#else
+#define EMPI_GLOBAL __global__
+#endif
 
 namespace empi {
 
@@ -44,9 +55,9 @@ __device__ __forceinline__ void refresh_stats(const DictPlan& dp, const ScalePla
 // of the previous subtraction (src/classes.cpp:67-70), then the dirty range of
 // every scale from the subtracted atom (src/gabor.cpp:197-208).  SCHED_ATOM:
 // dirty ranges of the atom (tA, sA) given by the caller.
-__global__ void k_sched_a(BatchDev b, int mode, int only_scale, double tA_in, double sA_in) {
+__device__ __forceinline__ void sched_a_inst(const BatchDev& b, int inst, int mode, int only_scale, double tA_in,
+                                             double sA_in) {
     const int init = mode == SCHED_INIT;
-    const int inst = blockIdx.x;
     const InstPlan ip = b.insts[inst];
     const DictPlan dp = b.dicts[ip.dict];
     __shared__ int s_active;
@@ -223,9 +234,13 @@ __global__ void k_sched_a(BatchDev b, int mode, int only_scale, double tA_in, do
     }
 }
 
-// Single CTA: exclusive scan of per-instance unit and chunk totals; resets the
-// work queues and candidate lists.
-__global__ void k_sched_b(BatchDev b) {
+EMPI_GLOBAL void k_sched_a(BatchDev b, int mode, int only_scale, double tA_in, double sA_in) {
+    sched_a_inst(b, blockIdx.x, mode, only_scale, tA_in, sA_in);
+}
+
+// Single CTA (any size up to 1024 threads): exclusive scan of per-instance
+// unit and chunk totals; resets the work queues and candidate lists.
+__device__ __forceinline__ void sched_b_block(const BatchDev& b) {
     __shared__ int s_u[1024], s_c[1024], s_a[1024];
     const int T = blockDim.x, tid = threadIdx.x;
     const int per = (b.ninst + T - 1) / T;
@@ -277,15 +292,18 @@ __global__ void k_sched_b(BatchDev b) {
     }
 }
 
+EMPI_GLOBAL void k_sched_b(BatchDev b) { sched_b_block(b); }
+
 // ------------------------------------------------------------ tournament tree
 
 // Leaf chunks: max over kChunk slot keys, re-keyed by slot index.
-__global__ void k_tree(BatchDev b) {
+// (blocks bid of nb: a fixed chunk per warp and stride, no work-queue atomic
+// per chunk)
+__device__ __forceinline__ void tree_body(const BatchDev& b, int bid, int nb) {
     const int lane = threadIdx.x & 31;
     const int total = b.ctr[CTR_TOTAL_CHUNKS];
-    // a fixed chunk per warp and stride: no work-queue atomic per chunk
-    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
-    for (int item = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); item < total; item += nwarps) {
+    const int nwarps = (int)((nb * blockDim.x) >> 5);
+    for (int item = (int)((bid * blockDim.x + threadIdx.x) >> 5); item < total; item += nwarps) {
         const int inst = upper_index(b.inst_chunks, b.ninst, item);
         int rem = item - b.inst_chunks[inst];
         const InstPlan ip = b.insts[inst];
@@ -317,6 +335,8 @@ __global__ void k_tree(BatchDev b) {
         }
     }
 }
+
+EMPI_GLOBAL void k_tree(BatchDev b) { tree_body(b, blockIdx.x, gridDim.x); }
 
 // ------------------------------------------------------------ proposal-ceiling probe
 //
@@ -355,7 +375,7 @@ __device__ __forceinline__ void for_dirty_slots(const BatchDev& b, F&& f) {
     }
 }
 
-__global__ void k_propagate(BatchDev b) {
+EMPI_GLOBAL void k_propagate(BatchDev b) {
     for_dirty_slots(b, [&](int inst, const InstPlan& ip, const DictPlan& dp, const ScalePlan& sp, int, long long s) {
         const InstState& st = b.state[inst];
         if (st.it < 1) return;
@@ -373,7 +393,7 @@ __global__ void k_propagate(BatchDev b) {
     });
 }
 
-__global__ void k_probe(BatchDev b) {
+EMPI_GLOBAL void k_probe(BatchDev b) {
     __shared__ double red[4][32];
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for_dirty_slots(b, [&](int inst, const InstPlan& ip, const DictPlan& dp, const ScalePlan& sp, int, long long s) {
@@ -417,7 +437,7 @@ __global__ void k_probe(BatchDev b) {
 
 // Heuristic proposer (a baseline for the learned one): the blocks nearest, in
 // (band, tile) steps, to the block of the atom just subtracted.
-__global__ void k_scores_last_atom(BatchDev b) {
+EMPI_GLOBAL void k_scores_last_atom(BatchDev b) {
     const int inst = blockIdx.x;
     const InstState& st = b.state[inst];
     const InstPlan ip = b.insts[inst];
@@ -436,7 +456,7 @@ __global__ void k_scores_last_atom(BatchDev b) {
 
 // per instance: the top prop_k blocks of the scores, then per scale the hull of
 // the selected tiles of its band as a t-range
-__global__ void k_topk_ranges(BatchDev b) {
+EMPI_GLOBAL void k_topk_ranges(BatchDev b) {
     __shared__ float s_sc[kProposalBlocks];
     __shared__ unsigned s_sel[kPropBands];
     __shared__ unsigned long long red[32];
@@ -497,7 +517,7 @@ __device__ __forceinline__ double atom_increment(const BatchDev& b, const InstPl
 
 __device__ __forceinline__ bool in_range(int2 r, int t) { return t >= r.x && t <= r.y; }
 
-__global__ void k_propagate_stale(BatchDev b) {
+EMPI_GLOBAL void k_propagate_stale(BatchDev b) {
     for_dirty_slots(b, [&](int inst, const InstPlan& ip, const DictPlan& dp, const ScalePlan& sp, int j, long long s) {
         const InstState& st = b.state[inst];
         const int t = (int)((s - sp.slot_base) / sp.G);
@@ -514,7 +534,7 @@ __global__ void k_propagate_stale(BatchDev b) {
 }
 
 // per instance: the largest certified lower bound of any slot after round 1
-__global__ void k_root(BatchDev b) {
+EMPI_GLOBAL void k_root(BatchDev b) {
     __shared__ unsigned long long red[32];
     const int inst = blockIdx.x;
     InstState& st = b.state[inst];
@@ -531,7 +551,7 @@ __global__ void k_root(BatchDev b) {
 // certified lower bound: a warp per leaf chunk over all instances' chunks,
 // skipping chunks whose maximum is below it.  Qualifying windows widen their
 // scale's round-2 range.
-__global__ void k_qualify(BatchDev b, int total_chunks) {
+EMPI_GLOBAL void k_qualify(BatchDev b, int total_chunks) {
     const int lane = threadIdx.x & 31;
     const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
     for (int item = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); item < total_chunks; item += nwarps) {
@@ -563,7 +583,7 @@ __global__ void k_qualify(BatchDev b, int total_chunks) {
 }
 
 // per instance: round 2's units, the hull of the qualifying windows per scale
-__global__ void k_round2_sched(BatchDev b) {
+EMPI_GLOBAL void k_round2_sched(BatchDev b) {
     const int inst = blockIdx.x;
     const InstPlan ip = b.insts[inst];
     const DictPlan dp = b.dicts[ip.dict];
@@ -603,11 +623,10 @@ __global__ void k_round2_sched(BatchDev b) {
 // leaf chunk), and the largest L among the candidates becomes the instance's
 // threshold tstar for the bins (k_collect).  No slot
 // outside the candidates can hold the exact maximum, whatever the FP32 error.
-__global__ void k_cand_slots(BatchDev b) {
+__device__ __forceinline__ void cand_slots_inst(const BatchDev& b, int inst) {
     __shared__ unsigned long long red[32];
     __shared__ unsigned long long s_root;
     __shared__ unsigned s_tstar;
-    const int inst = blockIdx.x;
     InstState& st = b.state[inst];
     if (st.status != ST_RUNNING) return;
     const InstPlan ip = b.insts[inst];
@@ -663,9 +682,11 @@ __global__ void k_cand_slots(BatchDev b) {
     if (threadIdx.x == 0) st.tstar = __float_as_uint(__uint_as_float(s_tstar) * (1.0f - b.band));
 }
 
+EMPI_GLOBAL void k_cand_slots(BatchDev b) { cand_slots_inst(b, blockIdx.x); }
+
 // FP64 value of one candidate bin and channel by direct DFT over its window
 // (GaborWorkspaceMap::compute, src/gabor.cpp:279-299, in FP64).
-__global__ void k_rescore(BatchDev b) {
+__device__ __forceinline__ void rescore_body(const BatchDev& b) {
     __shared__ double2 red[32];
     __shared__ int s_item;
     const int nb = min(b.ctr[CTR_CBINS], b.cbin_cap);
@@ -742,6 +763,8 @@ __global__ void k_rescore(BatchDev b) {
     }
 }
 
+EMPI_GLOBAL void k_rescore(BatchDev b) { rescore_body(b); }
+
 // GaborComputer for one bin in FP64 (src/gabor.cpp:44-71), constraint first
 // for MMP1 at low frequency (src/mmp.cpp:9-21).  v is modified in place.
 struct Computer64 {
@@ -786,12 +809,23 @@ __device__ __forceinline__ double norm_real(const Computer64& q, double phase) {
 
 // One CTA per instance: FP64 energies of its candidate bins, argmax (ties to
 // the lowest (scale, t, f)), atom parameters (src/gabor.cpp:111-131).
-__global__ void k_select(BatchDev b) {
-    __shared__ double s_e[128];
-    __shared__ unsigned long long s_key[128];
-    __shared__ int s_bin[128];
+// (energy, key, bin) of the better candidate: larger energy, ties to the
+// lower (scale, t, f) key
+__device__ __forceinline__ void better_bin(double& e, unsigned long long& k, int& bin, double oe,
+                                           unsigned long long ok, int obin) {
+    if (oe > e || (oe == e && ok < k)) {
+        e = oe;
+        k = ok;
+        bin = obin;
+    }
+}
+
+// (any block size up to 1024 threads)
+__device__ __forceinline__ void select_inst(const BatchDev& b, int inst) {
+    __shared__ double s_e[32];
+    __shared__ unsigned long long s_key[32];
+    __shared__ int s_bin[32];
     __shared__ double s_angle;
-    const int inst = blockIdx.x;
     InstState& st = b.state[inst];
     if (st.status != ST_RUNNING) return;
     const InstPlan ip = b.insts[inst];
@@ -847,22 +881,21 @@ __global__ void k_select(BatchDev b) {
             bbin = bin;
         }
     }
-    s_e[threadIdx.x] = be;
-    s_key[threadIdx.x] = bk;
-    s_bin[threadIdx.x] = bbin;
-    __syncthreads();
-    for (int off = blockDim.x / 2; off; off >>= 1) {
-        if (threadIdx.x < off) {
-            const double oe = s_e[threadIdx.x + off];
-            const unsigned long long ok = s_key[threadIdx.x + off];
-            if (oe > s_e[threadIdx.x] || (oe == s_e[threadIdx.x] && ok < s_key[threadIdx.x])) {
-                s_e[threadIdx.x] = oe;
-                s_key[threadIdx.x] = ok;
-                s_bin[threadIdx.x] = s_bin[threadIdx.x + off];
-            }
-        }
-        __syncthreads();
+#pragma unroll
+    for (int off = 16; off; off >>= 1)
+        better_bin(be, bk, bbin, __shfl_down_sync(0xffffffffu, be, off), __shfl_down_sync(0xffffffffu, bk, off),
+                   __shfl_down_sync(0xffffffffu, bbin, off));
+    if ((threadIdx.x & 31) == 0) {
+        s_e[threadIdx.x >> 5] = be;
+        s_key[threadIdx.x >> 5] = bk;
+        s_bin[threadIdx.x >> 5] = bbin;
     }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) better_bin(be, bk, bbin, s_e[w], s_key[w], s_bin[w]);
+        s_bin[0] = bbin;
+    }
+    __syncthreads();
     const int win = s_bin[0];
     if (EMPI_BAD(win < 0 || win >= b.cbin_cap, 7)) return;
     const CandBin cb = b.cbins[win];
@@ -900,6 +933,8 @@ __global__ void k_select(BatchDev b) {
         atomicAdd(b.ctr + CTR_STAT_BINS, nbins);
     }
 }
+
+EMPI_GLOBAL void k_select(BatchDev b) { select_inst(b, blockIdx.x); }
 
 // ------------------------------------------------------------ residual
 
@@ -954,9 +989,9 @@ __device__ __forceinline__ double atom_sample(const AtomWindow& a, int i, double
 
 // One CTA per (instance, channel): residual -= atom (fit = false), then the
 // channel's energy sum(x^2)/fs (SingleSignal::computeEnergy, inc/base.hpp:39-46).
-__global__ void k_subtract(BatchDev b) {
+__device__ __forceinline__ void subtract_blk(const BatchDev& b, int blk) {
     __shared__ double red[33];
-    const int2 ic = b.blk_ic[blockIdx.x];
+    const int2 ic = b.blk_ic[blk];
     const int inst = ic.x, c = ic.y;
     const InstState& st = b.state[inst];
     if (st.status != ST_RUNNING) return;
@@ -989,11 +1024,13 @@ __global__ void k_subtract(BatchDev b) {
     }
 }
 
+EMPI_GLOBAL void k_subtract(BatchDev b) { subtract_blk(b, blockIdx.x); }
+
 // One CTA per (instance, channel): residual from the float32 input
 // (src/io.cpp:33 converts to double; MMP2 sums channels, src/mmp.cpp:24-32)
 // unless the caller wrote the residual itself, its energy, and the instance
 // state.
-__global__ void k_init(BatchDev b, int from_input) {
+EMPI_GLOBAL void k_init(BatchDev b, int from_input) {
     __shared__ double red[33];
     const int2 ic = b.blk_ic[blockIdx.x];
     const int inst = ic.x, c = ic.y;
@@ -1042,7 +1079,7 @@ __global__ void k_init(BatchDev b, int from_input) {
 
 // Resumes the instances a candidate overflow stalled, once the host has
 // grown the candidate buffers.
-__global__ void k_unstall(BatchDev b) {
+EMPI_GLOBAL void k_unstall(BatchDev b) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < b.ninst; i += gridDim.x * blockDim.x) {
         InstState& st = b.state[i];
         if (st.status == ST_STALLED) {
@@ -1056,7 +1093,7 @@ __global__ void k_unstall(BatchDev b) {
 
 // Workspace::subtractAtomFromSignal on one FP64 signal (src/gabor.cpp:143-187),
 // fit or not; a single CTA.  params (6) are updated in place when fitting.
-__global__ void k_subtract_signal(double* x, float* x32, int N, double fs, double* params, int fit) {
+EMPI_GLOBAL void k_subtract_signal(double* x, float* x32, int N, double fs, double* params, int fit) {
     __shared__ double red[33];
     double p[6];
     for (int k = 0; k < 6; ++k) p[k] = params[k];
@@ -1089,7 +1126,7 @@ __global__ void k_subtract_signal(double* x, float* x32, int N, double fs, doubl
 // MMP2 per-channel fit (src/mmp.cpp:36-43 with subtractAtomFromSignal's fit
 // branch, src/gabor.cpp:165-183): one CTA per (epoch, channel), atoms in
 // order, each projected on the channel's residual in FP64.
-__global__ void k_mmp2_fit(BatchDev b, const int2* fit_map, double* fit_atoms, int fit_cap) {
+EMPI_GLOBAL void k_mmp2_fit(BatchDev b, const int2* fit_map, double* fit_atoms, int fit_cap) {
     __shared__ double red[33];
     const int2 ec = fit_map[blockIdx.x];  // (instance of the channel sum, input channel)
     const int inst = ec.x, c = ec.y;

@@ -387,7 +387,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
     // strides, so one table lookup per window or job is followed by
     // rotations.
     for (int c = 0; c < ip.C; ++c) {
-        const float* __restrict__ x = b.residual32 + ip.res_off + (long long)c * dp.N;
+        const float* EMPI_RESTRICT_MUT x = b.residual32 + ip.res_off + (long long)c * dp.N;
         const float2 one = make_float2(1.f, 0.f);
         auto twist = [&](int n) -> float2 {
             if (g == 1) return __ldg(tw + ((n & (2 * L - 1)) << (12 - LOGL)));
@@ -415,7 +415,7 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
         // FFT of a pair the sum is conjugate-twisted and multiplied by W_L^{n'}.
         // t, t2 = the twists at n = np.
         auto load_point = [&](const int4& m, float cf, int np, float2 t, float2 t2, float2& a1, float2& a2) {
-            const float* __restrict__ xs = x + m.x;
+            const float* EMPI_RESTRICT_MUT xs = x + m.x;
             a1 = make_float2(0.f, 0.f);
             a2 = make_float2(0.f, 0.f);
             if (F == 1) {
@@ -423,8 +423,8 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
                 // no loop and no rotation of the twist to a next fold
                 const int i0 = 2 * np;
                 if (i0 < m.y) {
-                    const float x0 = __ldg(xs + i0);
-                    const float x1 = (i0 + 1 < m.y) ? __ldg(xs + i0 + 1) : 0.0f;
+                    const float x0 = ld_mut(xs + i0);
+                    const float x1 = (i0 + 1 < m.y) ? ld_mut(xs + i0 + 1) : 0.0f;
                     const float d0 = (float)(i0 - m.z) - cf;
                     const float y0 = d0 * aG2, y1 = (d0 + 1.0f) * aG2;
                     const float2 z = make_float2(x0 * exp2f(-y0 * y0), x1 * exp2f(-y1 * y1));
@@ -442,8 +442,8 @@ __device__ __forceinline__ void unit_body(const BatchDev& b, unsigned char* smem
             for (int mm = 0; mm < F; ++mm, n += L) {
                 const int i0 = 2 * n;
                 if (i0 >= m.y) break;
-                const float x0 = __ldg(xs + i0);
-                const float x1 = (i0 + 1 < m.y) ? __ldg(xs + i0 + 1) : 0.0f;
+                const float x0 = ld_mut(xs + i0);
+                const float x1 = (i0 + 1 < m.y) ? ld_mut(xs + i0 + 1) : 0.0f;
                 const float d0 = (float)(i0 - m.z) - cf;
                 const float y0 = d0 * aG2, y1 = (d0 + 1.0f) * aG2;
                 const float2 z = make_float2(x0 * exp2f(-y0 * y0), x1 * exp2f(-y1 * y1));
@@ -1016,16 +1016,14 @@ __device__ __forceinline__ void collect_body(const BatchDev& b, unsigned char* s
 // CTAs per SM at 64 registers a thread (the default); MINB = 1: one CTA per SM
 // at 128 registers, without spills (the "wide" variant the autotuner may pick
 // per size).
-template <int MODE, int LOGL, int MINB>
-__global__ void __launch_bounds__(kUnitThreads, MINB) k_refresh(BatchDev b) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int s_unit;
+template <int LOGL, int MODE>
+__device__ __forceinline__ void refresh_queue(const BatchDev& b, unsigned char* smem, int* s_unit) {
     const int total = min(b.lcount[LOGL], b.lcap[LOGL]);
-    const int4* __restrict__ list = b.units + b.loff[LOGL];
+    const int4* EMPI_RESTRICT_MUT list = b.units + b.loff[LOGL];
     for (;;) {
-        if (threadIdx.x == 0) s_unit = atomicAdd(b.lhead + LOGL, 1);
+        if (threadIdx.x == 0) *s_unit = atomicAdd(b.lhead + LOGL, 1);
         __syncthreads();
-        const int u = s_unit;
+        const int u = *s_unit;
         __syncthreads();
         if (u >= total) break;
         const int4 un = list[u];  // (instance, scale | group << 16, t_start, nwin)
@@ -1033,12 +1031,40 @@ __global__ void __launch_bounds__(kUnitThreads, MINB) k_refresh(BatchDev b) {
     }
 }
 
+template <int MODE, int LOGL, int MINB>
+__global__ void __launch_bounds__(kUnitThreads, MINB) k_refresh(BatchDev b) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_unit;
+    refresh_queue<LOGL, MODE>(b, smem, &s_unit);
+}
+
+// Every sub-FFT size's list in one pass, largest transforms first (the
+// persistent kernel's refresh phase); smem holds the largest layout.
+template <int MODE>
+__device__ __forceinline__ void refresh_all_sizes(const BatchDev& b, unsigned char* smem, int* s_unit) {
+#define EMPI_REFRESH_SIZE(LG) \
+    if (b.lcount[LG] > 0) refresh_queue<LG, MODE>(b, smem, s_unit);
+    EMPI_REFRESH_SIZE(12)
+    EMPI_REFRESH_SIZE(11)
+    EMPI_REFRESH_SIZE(10)
+    EMPI_REFRESH_SIZE(9)
+    EMPI_REFRESH_SIZE(8)
+    EMPI_REFRESH_SIZE(7)
+    EMPI_REFRESH_SIZE(6)
+    EMPI_REFRESH_SIZE(5)
+    EMPI_REFRESH_SIZE(4)
+    EMPI_REFRESH_SIZE(3)
+    EMPI_REFRESH_SIZE(2)
+    EMPI_REFRESH_SIZE(1)
+    EMPI_REFRESH_SIZE(0)
+#undef EMPI_REFRESH_SIZE
+}
+
 // FP32 recompute of the candidate slots (one window each), emitting every bin
 // whose certified upper bound reaches the instance's lower bound tstar.
 template <int MODE>
-__global__ void __launch_bounds__(kUnitThreads, 1) k_collect(BatchDev b) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int s_unit;
+__device__ __forceinline__ void collect_queue(const BatchDev& b, unsigned char* smem, int* s_unit_p) {
+    int& s_unit = *s_unit_p;
     const int total = min(b.ctr[CTR_CSLOTS], b.cslot_cap);
     for (;;) {
         if (threadIdx.x == 0) s_unit = atomicAdd(b.ctr + CTR_CSLOT_Q, 1);
@@ -1076,6 +1102,13 @@ __global__ void __launch_bounds__(kUnitThreads, 1) k_collect(BatchDev b) {
             default: break;
         }
     }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kUnitThreads, 1) k_collect(BatchDev b) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_unit;
+    collect_queue<MODE>(b, smem, &s_unit);
 }
 
 // The refresh and collect kernels of one variant mode, with their shared

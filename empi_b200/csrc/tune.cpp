@@ -7,7 +7,8 @@
 // "samples", "energy_error" -- and the tuned shape: "transform_cap" (largest
 // shared-memory sub-FFT), "iterations_per_graph" and "wide_mask" (bit lg set:
 // the refresh kernel of sub-FFT size 2^lg runs one 128-register CTA per SM
-// instead of two 64-register ones).  Other keys (timings, the GPU's name) are
+// instead of two 64-register ones), optionally "persistent" (1: the MP loop
+// runs as one persistent kernel per chunk of iterations, 0: as the CUDA graph).  Other keys (timings, the GPU's name) are
 // ignored.  The reader below accepts exactly this flat shape: objects of
 // string keys and number or string values inside one array.
 #include "tune.hpp"
@@ -161,6 +162,7 @@ bool tune_lookup(const char* path, const TuneKey& key, TuneParams& out, std::str
                         if (kv.count("transform_cap")) out.transform_cap = (int)kv["transform_cap"];
                         if (kv.count("iterations_per_graph")) out.iterations_per_graph = (int)kv["iterations_per_graph"];
                         if (kv.count("wide_mask")) out.wide_mask = (int)kv["wide_mask"];
+                        if (kv.count("persistent")) out.persistent = kv["persistent"] != 0.0 ? 1 : 0;
                         found = true;
                     }
                     if (c.eat(']')) break;

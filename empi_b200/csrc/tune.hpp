@@ -17,6 +17,7 @@ struct TuneParams {
     int transform_cap = 0;         // 0: keep the engine's
     int iterations_per_graph = 0;  // 0: keep the engine's
     int wide_mask = 0;             // bit lg: one 128-register CTA per SM for sub-FFT size 2^lg
+    int persistent = -1;           // 1 / 0: the persistent kernel on / off; -1: the engine's choice
 };
 
 // Looks `key` up in the cache file; false with a camelCase reason in err when

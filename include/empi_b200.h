@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define EMPI_B200_ABI_VERSION 2
+#define EMPI_B200_ABI_VERSION 3
 
 typedef enum {
     EMPI_OK = 0,
@@ -45,7 +45,8 @@ typedef enum {
     EMPI_ERR_CONFIG = 8,               /* configuration errors (src/empi.cpp:59-141) */
     EMPI_ERR_IO = 9,                   /* file errors (src/io.cpp) */
     EMPI_ERR_NO_DEVICE = 10,
-    EMPI_ERR_INTERNAL = 11
+    EMPI_ERR_INTERNAL = 11,
+    EMPI_ERR_DEVICE_WAIT_TIMEOUT = 12  /* deviceWaitTimeout: a bounded device-side wait ran out */
 } empi_status;
 
 /* MP variants, src/empi.cpp:114-130 */
@@ -76,6 +77,16 @@ typedef struct {
     const char* tune_cache;  /* autotuner cache file (empi_b200/autotune.py) or NULL: batches
                                 whose workload it holds take its tuned sub-FFT cap, iterations
                                 per graph and per-size refresh variants (copied at creation) */
+    int persistent;          /* run each chunk of MP iterations as one persistent cooperative
+                                kernel instead of the multi-kernel CUDA graph: -1 = when the batch
+                                is small (the default), 0 = never, 1 = whenever the batch allows it
+                                (not with timing, a block proposal, the probe or pair collection) */
+    int wait_limit_ms;       /* time limit of every device-side wait of the persistent kernel
+                                (0 = default, 1000 ms); a wait that runs out ends the run with
+                                EMPI_ERR_DEVICE_WAIT_TIMEOUT and leaves the context usable */
+    int test_unreachable_wait; /* test hook, 0 in production: nonzero makes every grid barrier of
+                                the persistent kernel wait for one block more than exist, so
+                                the first wait runs out */
 } empi_engine_opts;
 
 void empi_engine_opts_default(empi_engine_opts* opts);
@@ -121,7 +132,7 @@ empi_status empi_dictionary_error_bounds(const empi_dictionary* dict, double fs,
  * none. */
 empi_status empi_tune_lookup(const char* path, int mode, int channels, double fs, int samples,
                              double energy_error, int* transform_cap, int* iterations_per_graph,
-                             int* wide_mask);
+                             int* wide_mask, int* persistent);
 
 /* -------------------------------------------------- workspace (the seam) */
 
@@ -253,6 +264,7 @@ typedef struct {
     /* block proposal (empi_batch_set_proposal): iterations that used one, and
      * how many of their atoms lay in a proposed block (the hit rate) */
     int proposal_iterations, proposal_hits;
+    int persistent;           /* 1: the run's MP iterations ran as the persistent kernel */
 } empi_batch_stats;
 
 empi_status empi_batch_get_stats(empi_batch* batch, empi_batch_stats* stats);
@@ -286,6 +298,16 @@ empi_status empi_batch_set_proposal(empi_batch* batch, int source, int k, const 
  * (band * 32 + tile) -- and their total in count. */
 empi_status empi_batch_collect_pairs(empi_batch* batch, int enable);
 empi_status empi_batch_pairs(empi_batch* batch, int cap, float* spec, int* block, int* count);
+
+/* The device index of one MP loop (instance: 0 .. loops - 1 in batch order,
+ * an SMP channel or an MMP epoch), the counterpart of inspecting the
+ * reference's Heap (inc/heap.hpp:13-94): its slot keys (upper-bound float bits
+ * << 32 | lower-bound float bits) and its tournament tree's leaf chunks
+ * (chunks: upper bits << 32 | slot index of the chunk's maximum; chunk_l: the
+ * chunk's largest lower bound).  Pass null arrays to get the sizes only. */
+empi_status empi_batch_tree(empi_batch* batch, int instance, long long slot_cap, unsigned long long* slots,
+                            long long* slot_count, int chunk_cap, unsigned long long* chunks, unsigned* chunk_l,
+                            int* chunk_count);
 
 /* The proposal network on a GPU, host arrays in and out (no counterpart in
  * the reference).  Weights: empi_proposal_parameter_count() floats in the

@@ -28,7 +28,7 @@ def test_library_exports_every_declared_function():
     for n in names:
         assert hasattr(L, n), n
     assert set(names) == set(empi_b200.EXPORTS)
-    assert L.empi_abi_version() == 2
+    assert L.empi_abi_version() == 3
 
 
 @pytest.mark.parametrize("fs,n,eps", [(128.0, 1280, 0.01), (256.0, 5120, 0.01), (512.0, 16384, 0.005),
@@ -134,8 +134,10 @@ def test_tune_cache_lookup(tmp_path):
     autotune.write_cache(str(path), e1)
     autotune.write_cache(str(path), e2)
     autotune.write_cache(str(path), dict(e1, wide_mask=4))  # replaces e1
-    assert empi_b200.tune_lookup(str(path), 0, 1, 256.0, 5120, 0.01) == (2048, 16, 4)
-    assert empi_b200.tune_lookup(str(path), 0, 1, 256.0, 0, 0.01) == (1024, 4, 0)
+    assert empi_b200.tune_lookup(str(path), 0, 1, 256.0, 5120, 0.01) == (2048, 16, 4, -1)
+    assert empi_b200.tune_lookup(str(path), 0, 1, 256.0, 0, 0.01) == (1024, 4, 0, -1)
+    autotune.write_cache(str(path), dict(e2, persistent=1))
+    assert empi_b200.tune_lookup(str(path), 0, 1, 256.0, 0, 0.01) == (1024, 4, 0, 1)
     assert empi_b200.tune_lookup(str(path), 3, 1, 256.0, 5120, 0.01) is None
     assert empi_b200.tune_lookup(str(path), 0, 1, 256.0, 5120, 0.02) is None
     bad = tmp_path / "bad.json"

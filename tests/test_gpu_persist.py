@@ -1,0 +1,113 @@
+"""The persistent MP-loop kernel (persist.cuh) against the multi-kernel graph
+and the reference.
+
+* Every reference golden (tests/golden/cases.json) decomposed with the
+  persistent kernel forced on and forced off: the atoms, indices and residual
+  energies are bit-identical, and match the reference's.
+* Uneven batches with stalls on candidate overflow (buffers regrown between
+  chunks) give the graph's atoms.
+* Failure detection without a GPU fault: a test hook makes every grid barrier
+  wait for one block more than the grid holds; the bounded wait runs out, the
+  run returns deviceWaitTimeout, and the device stays usable for the next
+  decomposition.
+"""
+import numpy as np
+import pytest
+
+import empi_b200
+from empi_b200 import synth
+from helpers import case_limits, case_signal, compare_sequences, golden
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+CASES = golden()["cases"]
+
+
+@pytest.fixture(scope="module")
+def engines():
+    on = empi_b200.Engine(persistent=1)
+    off = empi_b200.Engine(persistent=0)
+    yield on, off
+    on.close()
+    off.close()
+
+
+def run(variant, epochs, fs, eps, iters, percent, engine, lim=None):
+    lim = lim or dict(smin=0.0, smax=float("inf"), fmax=float("inf"))
+    settings = empi_b200.DecompositionSettings(int(iters), 1.0 - 0.01 * float(percent))
+    b = empi_b200.Batch(variant, eps, settings, [e.shape for e in epochs], fs, lim["smin"], lim["smax"], lim["fmax"],
+                        engine=engine)
+    b.load(epochs)
+    b.run()
+    st = b.stats()
+    res = [b.result(e) for e in range(len(epochs))]
+    b.close()
+    return res, st
+
+
+def assert_identical(a, b):
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x.counts, y.counts)
+        np.testing.assert_array_equal(x.indices, y.indices)
+        np.testing.assert_array_equal(x.atoms, y.atoms)
+        np.testing.assert_array_equal(x.energies, y.energies)
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_persistent_equals_graph_and_reference(engines, case):
+    on, off = engines
+    fs, x = case_signal(case)
+    lim = case_limits(case)
+    args = (case["variant"], [x], fs, case["energy_error"], case["iterations"], case["energy_percent"])
+    got, st_on = run(*args, on, lim)
+    ref_graph, st_off = run(*args, off, lim)
+    assert st_on.persistent == 1 and st_off.persistent == 0
+    assert_identical(got, ref_graph)
+    ora = O.decompose(case["variant"], fs, x.T.astype(np.float64), case["energy_error"], case["iterations"],
+                      case["energy_percent"], **lim)
+    smp = case["variant"] == "smp" or x.shape[1] == 1
+    res = got[0]
+    for c in range(x.shape[1]):
+        e_got = res.energies[c] if smp else res.energies
+        compare_sequences(case["atoms"][c], res.atoms[c, : res.counts[c]], ora.margins[c if smp else 0],
+                          case["energies"][c if smp else 0] if case["variant"] != "mmp2" or c == 0 else None,
+                          e_got, label=f"{case['name']} ch{c} persistent")
+    print(f"{case['name']}: persistent {st_on.run_ms:.2f} ms ({st_on.kernel_launches} launches), "
+          f"graph {st_off.run_ms:.2f} ms ({st_off.kernel_launches} launches)")
+
+
+@pytest.mark.parametrize("variant", ["smp", "mmp2", "mmp3"])
+def test_persistent_uneven_batch_and_regrowth(variant):
+    """An uneven batch (instances stopping at different iterations) and a
+    candidate capacity small enough that instances stall and the buffers
+    regrow between chunks."""
+    w = synth.workload(3, epochs=5, seed=3)
+    eps = [e[:, :2] for e in w.epochs]
+    outs = []
+    for pers in (1, 0):
+        eng = empi_b200.Engine(persistent=pers, candidate_capacity=4)
+        res, st = run(variant, eps, w.fs, w.energy_error, 20, 99.0, eng)
+        assert st.persistent == pers
+        outs.append(res)
+        eng.close()
+    assert_identical(outs[0], outs[1])
+
+
+def test_wait_that_runs_out_returns_device_wait_timeout():
+    w = synth.workload(0)
+    x = w.epochs[0]
+    hung = empi_b200.Engine(persistent=1, wait_limit_ms=50, test_unreachable_wait=True)
+    with pytest.raises(empi_b200.EmpiError) as ei:
+        run("smp", [x], w.fs, w.energy_error, 10, 100.0, hung)
+    assert ei.value.status == 12 and ei.value.message.startswith("deviceWaitTimeout")
+    hung.close()
+    # the context is still usable: the same decomposition, persistent and graph
+    ok = empi_b200.Engine(persistent=1)
+    a, st = run("smp", [x], w.fs, w.energy_error, 10, 100.0, ok)
+    ok.close()
+    g = empi_b200.Engine(persistent=0)
+    b, _ = run("smp", [x], w.fs, w.energy_error, 10, 100.0, g)
+    g.close()
+    assert st.persistent == 1
+    assert_identical(a, b)
