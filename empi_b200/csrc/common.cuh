@@ -31,7 +31,8 @@ enum Counter {
     CTR_CHECK = 13,      // (EMPI_CHECK builds) largest code of a failed bounds check
     CTR_PROP_ITERS = 14, // block proposal: iterations that used it
     CTR_PROP_HITS = 15,  // ... and whose atom lay in a proposed block
-    CTR_COUNT = 16
+    CTR_PACTIVE = 16,    // persistent kernel: instances still running, by iteration parity (two words)
+    CTR_COUNT = 18
 };
 
 // Block proposal geometry: 16 scale bands (scale j of n falls in band

@@ -78,7 +78,11 @@ extern "C" const char* empi_status_string(empi_status st) {
 // ------------------------------------------------------------ engine
 
 constexpr int kSizes = kRefreshSizes;  // sub-FFT sizes 2^0 .. 2^12, one refresh kernel each
-constexpr long long kPersistAutoSlots = 1LL << 19;  // batches up to this many slot keys run persistent
+// batches whose slot keys x channels per MP loop stay within this run the
+// persistent kernel by default (measured on a B200: 0.70-0.89x of the graph's
+// time at 4.6k-32k, equal at 69k, 1.1-1.45x slower from 75k on, where each
+// per-instance step's own latency, not launch latency, bounds an iteration)
+constexpr long long kPersistAutoWork = 1LL << 15;
 
 struct empi_engine {
     empi_engine_opts opts;
@@ -363,7 +367,8 @@ struct empi_batch {
     int launches_per_iter = 10;
     int regrows = 0;  // candidate-buffer growths (overflow recoveries) so far
     int total_chunks = 0;  // leaf chunks of all instances
-    long long total_slots = 0;  // slot keys of all instances
+    long long total_slots = 0;      // slot keys of all instances
+    long long total_slot_work = 0;  // ... each times its MP loop's channels
 
     ~empi_batch() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -416,14 +421,22 @@ empi_status configure(empi_batch* b) {
     // faster).  It needs one co-resident 512-thread CTA per SM.
     int want = b->eng->opts.persistent;
     if (want < 0) want = b->tuned_persistent;
-    if (want < 0) want = (long long)b->total_slots <= kPersistAutoSlots ? 1 : 0;
+    if (want < 0) want = b->total_slot_work <= kPersistAutoWork ? 1 : 0;
     b->persistent = false;
     int coop = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, b->eng->device));
     if (want == 1 && coop && rk.persist) {
+        // the largest refresh layout plus the phases' static shared memory
+        // must fit one CTA (MMP1's per-bin channel sums at small L do not)
+        cudaFuncAttributes fa{};
+        int optin = 0;
+        CUDA_TRY(cudaFuncGetAttributes(&fa, rk.persist));
+        CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->eng->device));
         int o = 0;
-        CUDA_TRY(cudaFuncSetAttribute(rk.persist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk.persist_smem));
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, rk.persist, kUnitThreads, rk.persist_smem) ==
+        if (fa.sharedSizeBytes + rk.persist_smem <= (size_t)optin &&
+            cudaFuncSetAttribute(rk.persist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rk.persist_smem) ==
+                cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, rk.persist, kUnitThreads, rk.persist_smem) ==
                 cudaSuccess &&
             o >= 1) {
             b->persistent = true;
@@ -514,6 +527,7 @@ void launch_proposal_update(empi_batch* b, cudaStream_t s, cudaEvent_t e0, cudaE
     k_qualify<<<b->tree_grid, 256, 0, s>>>(b->dev, b->total_chunks);
     cudaMemsetAsync(b->dev.lcount, 0, sizeof(int) * 2 * 16, s);
     k_round2_sched<<<ninst, 128, 0, s>>>(b->dev);
+    k_chunk_prefix<<<1, std::min(1024, 32 * ((ninst + 31) / 32)), 0, s>>>(b->dev);
     launch_refresh(b, s);
     if (e1) cudaEventRecord(e1, s);
     k_tree<<<b->tree_grid, 256, 0, s>>>(b->dev);
@@ -627,6 +641,7 @@ empi_status build_batch(empi_engine* eng, int variant, const empi_dictionary* di
             cen_off += C;
             res_off += (long long)C * dp.N;
             slot_off += dp.slots;
+            b->total_slot_work += dp.slots * C;
             chunk_off += dp.chunks;
             out_off += (long long)iters * C * 6;
             b->cmax = std::max(b->cmax, C);

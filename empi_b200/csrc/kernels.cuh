@@ -296,7 +296,39 @@ EMPI_GLOBAL void k_sched_b(BatchDev b) { sched_b_block(b); }
 
 // ------------------------------------------------------------ tournament tree
 
-// Leaf chunks: max over kChunk slot keys, re-keyed by slot index.
+// Leaf chunks: max over kChunk slot keys, re-keyed by slot index.  One warp:
+// the leaf chunk holding dirty chunk `rem` of instance inst (its scales' dirty
+// chunk ranges in order, prefix sums ij_chunks).
+__device__ __forceinline__ void tree_chunk(const BatchDev& b, int inst, int rem, int lane) {
+    const InstPlan ip = b.insts[inst];
+    const DictPlan dp = b.dicts[ip.dict];
+    const int j = upper_index(b.ij_chunks + ip.ij_off + inst, dp.nscales, rem);
+    rem -= ld_mut(b.ij_chunks + ip.ij_off + inst + j);
+    const int chunk = b.ij_crange[ip.ij_off + j].x + rem;
+    if (EMPI_BAD(chunk < 0 || chunk >= dp.chunks, 12)) return;
+    const long long s0 = (long long)chunk * kChunk;
+    const long long s1 = min(s0 + kChunk, dp.slots);
+    const unsigned long long* sl = b.slots + ip.slot_off;
+    unsigned long long best = 0;
+    unsigned bestl = 0;
+    for (long long s = s0 + lane; s < s1; s += 32) {
+        const unsigned long long v = sl[s];
+        const unsigned long long key = (v & 0xffffffff00000000ull) | (unsigned long long)(s);
+        best = key > best ? key : best;
+        bestl = max(bestl, (unsigned)(v & 0xffffffffull));
+    }
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+        unsigned long long o = __shfl_down_sync(0xffffffffu, best, off);
+        best = o > best ? o : best;
+    }
+    bestl = __reduce_max_sync(0xffffffffu, bestl);
+    if (lane == 0) {
+        b.chunks[ip.chunk_off + chunk] = best;
+        b.chunk_l[ip.chunk_off + chunk] = bestl;
+    }
+}
+
 // (blocks bid of nb: a fixed chunk per warp and stride, no work-queue atomic
 // per chunk)
 __device__ __forceinline__ void tree_body(const BatchDev& b, int bid, int nb) {
@@ -305,35 +337,17 @@ __device__ __forceinline__ void tree_body(const BatchDev& b, int bid, int nb) {
     const int nwarps = (int)((nb * blockDim.x) >> 5);
     for (int item = (int)((bid * blockDim.x + threadIdx.x) >> 5); item < total; item += nwarps) {
         const int inst = upper_index(b.inst_chunks, b.ninst, item);
-        int rem = item - b.inst_chunks[inst];
-        const InstPlan ip = b.insts[inst];
-        const DictPlan dp = b.dicts[ip.dict];
-        const int j = upper_index(b.ij_chunks + ip.ij_off + inst, dp.nscales, rem);
-        rem -= b.ij_chunks[ip.ij_off + inst + j];
-        const int chunk = b.ij_crange[ip.ij_off + j].x + rem;
-        if (EMPI_BAD(chunk < 0 || chunk >= dp.chunks, 12)) continue;
-        const long long s0 = (long long)chunk * kChunk;
-        const long long s1 = min(s0 + kChunk, dp.slots);
-        const unsigned long long* sl = b.slots + ip.slot_off;
-        unsigned long long best = 0;
-        unsigned bestl = 0;
-        for (long long s = s0 + lane; s < s1; s += 32) {
-            const unsigned long long v = sl[s];
-            const unsigned long long key = (v & 0xffffffff00000000ull) | (unsigned long long)(s);
-            best = key > best ? key : best;
-            bestl = max(bestl, (unsigned)(v & 0xffffffffull));
-        }
-#pragma unroll
-        for (int off = 16; off; off >>= 1) {
-            unsigned long long o = __shfl_down_sync(0xffffffffu, best, off);
-            best = o > best ? o : best;
-        }
-        bestl = __reduce_max_sync(0xffffffffu, bestl);
-        if (lane == 0) {
-            b.chunks[ip.chunk_off + chunk] = best;
-            b.chunk_l[ip.chunk_off + chunk] = bestl;
-        }
+        tree_chunk(b, inst, item - ld_mut(b.inst_chunks + inst), lane);
     }
+}
+
+// The dirty leaf chunks of one instance, by the warps of one CTA (the
+// persistent kernel's tree step).
+__device__ __forceinline__ void tree_inst(const BatchDev& b, int inst) {
+    const InstPlan ip = b.insts[inst];
+    const int total = ld_mut(b.ij_chunks + ip.ij_off + inst + b.dicts[ip.dict].nscales);
+    for (int item = (int)(threadIdx.x >> 5); item < total; item += (int)(blockDim.x >> 5))
+        tree_chunk(b, inst, item, threadIdx.x & 31);
 }
 
 EMPI_GLOBAL void k_tree(BatchDev b) { tree_body(b, blockIdx.x, gridDim.x); }
@@ -604,11 +618,63 @@ EMPI_GLOBAL void k_round2_sched(BatchDev b) {
                 if (at < cap) list[at] = make_int4(inst, j | (g << 16), t0, min(B, q.y - t0 + 1));
         }
         refresh_stats(dp, sp, ip.C, q.x, q.y, st_flops, st_bytes, st_slots);
+        // the leaf chunks the tree re-reduces after round 2: the dirty range's
+        // and the hull's (stale slots of earlier iterations lie outside the
+        // dirty range), as one covering range
+        int c0 = (int)((sp.slot_base + (long long)q.x * sp.G) / kChunk);
+        int c1 = (int)((sp.slot_base + (long long)(q.y + 1) * sp.G - 1) / kChunk);
+        const int2 cr = b.ij_crange[ip.ij_off + j];
+        if (cr.y > 0) {
+            c0 = min(c0, cr.x);
+            c1 = max(c1, cr.x + cr.y - 1);
+        }
+        b.ij_crange[ip.ij_off + j] = make_int2(c0, c1 - c0 + 1);
     }
     if (st_flops != 0.0) {
         atomicAdd(b.stats + 0, st_flops);
         atomicAdd(b.stats + 1, st_bytes);
         atomicAdd(b.stats + 2, st_slots);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {  // the instance's chunk prefix over scales (k_tree's index)
+        int* chunks = b.ij_chunks + ip.ij_off + inst;
+        int acc = 0;
+        for (int j = 0; j < dp.nscales; ++j) {
+            acc += b.ij_crange[ip.ij_off + j].y;
+            chunks[j + 1] = acc;
+        }
+    }
+}
+
+// Single CTA: the chunk prefix over instances after round 2 widened their
+// chunk ranges (the chunk part of k_sched_b).
+EMPI_GLOBAL void k_chunk_prefix(BatchDev b) {
+    __shared__ int s_c[1024];
+    const int T = blockDim.x, tid = threadIdx.x;
+    const int per = (b.ninst + T - 1) / T;
+    const int i0 = tid * per, i1 = min(b.ninst, i0 + per);
+    int sc = 0;
+    for (int i = i0; i < i1; ++i) {
+        const InstPlan ip = b.insts[i];
+        sc += b.ij_chunks[ip.ij_off + i + b.dicts[ip.dict].nscales];
+    }
+    s_c[tid] = sc;
+    __syncthreads();
+    for (int off = 1; off < T; off <<= 1) {
+        const int v = tid >= off ? s_c[tid - off] : 0;
+        __syncthreads();
+        s_c[tid] += v;
+        __syncthreads();
+    }
+    int pc = tid ? s_c[tid - 1] : 0;
+    for (int i = i0; i < i1; ++i) {
+        const InstPlan ip = b.insts[i];
+        b.inst_chunks[i] = pc;
+        pc += b.ij_chunks[ip.ij_off + i + b.dicts[ip.dict].nscales];
+    }
+    if (tid == T - 1) {
+        b.inst_chunks[b.ninst] = s_c[T - 1];
+        b.ctr[CTR_TOTAL_CHUNKS] = s_c[T - 1];
     }
 }
 
@@ -989,10 +1055,8 @@ __device__ __forceinline__ double atom_sample(const AtomWindow& a, int i, double
 
 // One CTA per (instance, channel): residual -= atom (fit = false), then the
 // channel's energy sum(x^2)/fs (SingleSignal::computeEnergy, inc/base.hpp:39-46).
-__device__ __forceinline__ void subtract_blk(const BatchDev& b, int blk) {
+__device__ __forceinline__ void subtract_ic(const BatchDev& b, int inst, int c) {
     __shared__ double red[33];
-    const int2 ic = b.blk_ic[blk];
-    const int inst = ic.x, c = ic.y;
     const InstState& st = b.state[inst];
     if (st.status != ST_RUNNING) return;
     const InstPlan ip = b.insts[inst];
@@ -1022,6 +1086,11 @@ __device__ __forceinline__ void subtract_blk(const BatchDev& b, int blk) {
         b.chan_energy[ip.cen_off + c] = s / fs;
         b.chan_xmax[ip.cen_off + c] = xm;
     }
+}
+
+__device__ __forceinline__ void subtract_blk(const BatchDev& b, int blk) {
+    const int2 ic = b.blk_ic[blk];
+    subtract_ic(b, ic.x, ic.y);
 }
 
 EMPI_GLOBAL void k_subtract(BatchDev b) { subtract_blk(b, blockIdx.x); }

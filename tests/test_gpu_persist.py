@@ -2,8 +2,9 @@
 and the reference.
 
 * Every reference golden (tests/golden/cases.json) decomposed with the
-  persistent kernel forced on and forced off: the atoms, indices and residual
-  energies are bit-identical, and match the reference's.
+  persistent kernel forced on and forced off: the atoms and indices are
+  bit-identical, the residual energies equal to 1e-13, and both match the
+  reference's.
 * Uneven batches with stalls on candidate overflow (buffers regrown between
   chunks) give the graph's atoms.
 * Failure detection without a GPU fault: a test hook makes every grid barrier
@@ -47,11 +48,14 @@ def run(variant, epochs, fs, eps, iters, percent, engine, lim=None):
 
 
 def assert_identical(a, b):
+    """Atoms bit-identical; residual energies to the last bits (the FP64
+    energy sum runs over 512 threads in the persistent kernel and 1024 in the
+    graph's subtraction kernel, so its addition order differs)."""
     for x, y in zip(a, b):
         np.testing.assert_array_equal(x.counts, y.counts)
         np.testing.assert_array_equal(x.indices, y.indices)
         np.testing.assert_array_equal(x.atoms, y.atoms)
-        np.testing.assert_array_equal(x.energies, y.energies)
+        np.testing.assert_allclose(x.energies, y.energies, rtol=1e-13, atol=0)
 
 
 @pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
@@ -62,7 +66,9 @@ def test_persistent_equals_graph_and_reference(engines, case):
     args = (case["variant"], [x], fs, case["energy_error"], case["iterations"], case["energy_percent"])
     got, st_on = run(*args, on, lim)
     ref_graph, st_off = run(*args, off, lim)
-    assert st_on.persistent == 1 and st_off.persistent == 0
+    # MMP1's shared-memory layout (per-bin channel sums) leaves no room for the
+    # persistent kernel's: its engine falls back to the graph
+    assert st_off.persistent == 0 and st_on.persistent == (0 if case["variant"] == "mmp1" else 1)
     assert_identical(got, ref_graph)
     ora = O.decompose(case["variant"], fs, x.T.astype(np.float64), case["energy_error"], case["iterations"],
                       case["energy_percent"], **lim)
