@@ -225,6 +225,19 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
+def profiled_executed_fp32(w):
+    """Executed FP32 FLOPs of the refresh as a fraction of the FP32 peak, from
+    the committed ncu figure (profiles/refresh_traffic_mmp2_19x8x5120.json);
+    None for other workloads."""
+    if w.name != "mmp2-19x8x5120@256":
+        return None
+    try:
+        with open(os.path.join(ROOT, "profiles", "refresh_traffic_mmp2_19x8x5120.json")) as f:
+            return float(json.load(f)["executed_fp32_frac_of_peak"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
 def profiled_traffic(w):
     """DRAM bytes of one refresh fork of the headline workload from the
     committed ncu figure (profiles/refresh_traffic_mmp2_19x8x5120.json);
@@ -393,7 +406,11 @@ def ours(args):
         roofline_fp32 = {"achieved": flops_per_launch / (per_launch_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
                          "peak": fp32_peak, "peak_source": "nominal FP32 CUDA-core (148 SMs x 128 x 2 x 1.965 GHz)",
                          "frac": flops_per_launch / (per_launch_ms * 1e-3) / 1e12 / fp32_peak,
-                         "flops": "reference-equivalent 2.5 Nfft log2 Nfft per refreshed window"}
+                         "flops": "reference-equivalent 2.5 Nfft log2 Nfft per refreshed window",
+                         "executed_frac": profiled_executed_fp32(w),
+                         "executed_source": "ncu FP32 thread instructions of k_refresh<0, 12, 2> (profiles/"
+                                            "refresh_traffic_mmp2_19x8x5120.json)" if profiled_executed_fp32(w)
+                                            else None}
     bt.close()
     eng_t.close()
 

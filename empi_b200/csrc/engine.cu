@@ -330,7 +330,7 @@ struct empi_batch {
     DevBuf<float> d_dump, d_prop, d_pscores;
     DevBuf<double> d_probe;
     DevBuf<int2> d_prange, d_qrange;
-    DevBuf<unsigned char> d_stale;
+    DevBuf<unsigned char> d_stale, d_qmark;
     int prop_source = -1;  // block proposal: 0 learned network, 1 last-atom heuristic, 2 none (k = 0)
     ProposalNet net;       // the learned proposer's device weights and activations
     DevBuf<float> d_pairs; // training-pair collection: [instance][iteration][64 x 128] spectrograms
@@ -1001,6 +1001,7 @@ empi_status batch_run_hooked(empi_batch* b, const std::function<void()>& after_c
     CUDA_TRY(cudaMemsetAsync(b->d_ctr.p, 0, sizeof(int) * CTR_COUNT, s));
     CUDA_TRY(cudaMemsetAsync(b->d_stats.p, 0, sizeof(double) * 4, s));
     if (b->dev.probe) CUDA_TRY(cudaMemsetAsync(b->dev.probe, 0, sizeof(double) * 4, s));
+    if (b->dev.qmark) CUDA_TRY(cudaMemsetAsync(b->dev.qmark, 0, b->d_qmark.n, s));
     CUDA_TRY(cudaMemsetAsync(b->d_energies.p, 0xff, sizeof(double) * b->d_energies.n, s));  // NaN
     CUDA_TRY(cudaEventRecord(b->run_start, s));
     k_init<<<(int)b->blk_ic.size(), 256, 0, s>>>(b->dev, 1);
@@ -1148,6 +1149,7 @@ extern "C" empi_status empi_batch_set_proposal(empi_batch* b, int source, int k,
         b->dev.prange = nullptr;
         b->dev.qrange = nullptr;
         b->dev.stale = nullptr;
+        b->dev.qmark = nullptr;
         return ok();
     }
     if (source == 0) {
@@ -1168,6 +1170,9 @@ extern "C" empi_status empi_batch_set_proposal(empi_batch* b, int source, int k,
     if (!b->d_stale.p) CUDA_TRY(b->d_stale.alloc(b->d_slots.n));
     CUDA_TRY(cudaMemset(b->d_stale.p, 0, b->d_stale.n));
     b->dev.stale = b->d_stale.p;
+    if (!b->d_qmark.p) CUDA_TRY(b->d_qmark.alloc(b->d_slots.n));
+    CUDA_TRY(cudaMemset(b->d_qmark.p, 0, b->d_qmark.n));
+    b->dev.qmark = b->d_qmark.p;
     return ok();
 }
 

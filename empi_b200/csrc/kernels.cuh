@@ -590,13 +590,31 @@ EMPI_GLOBAL void k_qualify(BatchDev b, int total_chunks) {
             if (!b.stale[ip.slot_off + s] || (unsigned)(b.slots[ip.slot_off + s] >> 32) < lb) continue;
             int j, t, g;
             slot_to_jtg(b, dp, s, j, t, g);
+            // mark the group's unit block holding t (on the block's first slot)
+            const ScalePlan& sp = b.scales[dp.scale0 + j];
+            const int B = g >= 2 ? sp.B2 : sp.B1;
+            b.qmark[ip.slot_off + sp.slot_base + (long long)(t / B) * B * sp.G + g] = 1;
             atomicMin(&b.qrange[ip.ij_off + j].x, t);
             atomicMax(&b.qrange[ip.ij_off + j].y, t);
         }
     }
 }
 
-// per instance: round 2's units, the hull of the qualifying windows per scale
+// refresh_stats for one residue group's slots of windows lo..hi: its share of
+// the window's transform work (1 or 2 of the M residues), its slot writes
+__device__ __forceinline__ void refresh_stats_group(const DictPlan& dp, const ScalePlan& sp, int C, int g, int lo,
+                                                    int hi, double& flops, double& bytes, double& slots) {
+    double f = 0.0, by = 0.0, sl = 0.0;
+    refresh_stats(dp, sp, C, lo, hi, f, by, sl);
+    const int n = hi - lo + 1;
+    flops += f * (sp.M == 1 ? 1.0 : (g >= 2 ? 2.0 : 1.0) / sp.M);
+    bytes += by - 8.0 * n * (sp.G - 1);
+    slots += n;
+}
+
+// per instance: round 2's units, exactly the unit blocks (per scale and
+// residue group, B windows aligned to B) that hold a qualifying slot; the
+// marks are cleared as the units are emitted
 EMPI_GLOBAL void k_round2_sched(BatchDev b) {
     const int inst = blockIdx.x;
     const InstPlan ip = b.insts[inst];
@@ -607,22 +625,29 @@ EMPI_GLOBAL void k_round2_sched(BatchDev b) {
         b.qrange[ip.ij_off + j] = make_int2(0x7fffffff, -1);
         if (q.y < q.x) continue;
         const ScalePlan sp = b.scales[dp.scale0 + j];
-        int nu = 0;
-        for (int g = 0; g < sp.G; ++g) nu += group_units(q.y - q.x + 1, g, sp);
-        int at = atomicAdd(b.lcount + sp.logL, nu);
         const int cap = b.lcap[sp.logL];
         int4* list = b.units + b.loff[sp.logL];
+        int tmin = 0x7fffffff, tmax = -1;
         for (int g = 0; g < sp.G; ++g) {
             const int B = g >= 2 ? sp.B2 : sp.B1;
-            for (int t0 = q.x; t0 <= q.y; t0 += B, ++at)
-                if (at < cap) list[at] = make_int4(inst, j | (g << 16), t0, min(B, q.y - t0 + 1));
+            for (int t0 = (q.x / B) * B; t0 <= q.y; t0 += B) {
+                unsigned char* mk = b.qmark + ip.slot_off + sp.slot_base + (long long)t0 * sp.G + g;
+                if (!*mk) continue;
+                *mk = 0;
+                const int n = min(B, sp.tcount - t0);
+                const int at = atomicAdd(b.lcount + sp.logL, 1);
+                if (at < cap) list[at] = make_int4(inst, j | (g << 16), t0, n);
+                refresh_stats_group(dp, sp, ip.C, g, t0, t0 + n - 1, st_flops, st_bytes, st_slots);
+                tmin = min(tmin, t0);
+                tmax = max(tmax, t0 + n - 1);
+            }
         }
-        refresh_stats(dp, sp, ip.C, q.x, q.y, st_flops, st_bytes, st_slots);
+        if (tmax < tmin) continue;
         // the leaf chunks the tree re-reduces after round 2: the dirty range's
-        // and the hull's (stale slots of earlier iterations lie outside the
-        // dirty range), as one covering range
-        int c0 = (int)((sp.slot_base + (long long)q.x * sp.G) / kChunk);
-        int c1 = (int)((sp.slot_base + (long long)(q.y + 1) * sp.G - 1) / kChunk);
+        // and the refreshed blocks' (stale slots of earlier iterations lie
+        // outside the dirty range), as one covering range
+        int c0 = (int)((sp.slot_base + (long long)tmin * sp.G) / kChunk);
+        int c1 = (int)((sp.slot_base + (long long)(tmax + 1) * sp.G - 1) / kChunk);
         const int2 cr = b.ij_crange[ip.ij_off + j];
         if (cr.y > 0) {
             c0 = min(c0, cr.x);
