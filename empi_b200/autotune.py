@@ -102,7 +102,6 @@ class _Trial:
             times.append(b.stats().run_ms)
         st = b.stats()
         assert st.tuned == 1 and st.transform_cap == shape["transform_cap"]
-        assert "persistent" not in shape or st.persistent == shape["persistent"]
         atoms = [b.result(e) for e in range(len(self.epochs))]
         b.close()
         eng.close()
@@ -127,7 +126,10 @@ def tune(variant, epochs, fs, energy_error, iterations, energy_percent, device=0
 
     def consider(cand):
         nonlocal best_t, best
-        t, _, atoms = trial.run(cand, reps)
+        t, st, atoms = trial.run(cand, reps)
+        if cand.get("persistent") == 1 and not st.persistent:
+            log(f"  {cand}: the persistent kernel does not fit this workload's layout")
+            return
         if not _same_atoms(atoms, ref_atoms):
             raise AssertionError(f"shape {cand} changed the atoms")
         better = t < best_t * 0.99

@@ -151,6 +151,7 @@ struct BatchDev {
     int prop_k;
     unsigned char* stale;  // block proposal: per slot, 1 while its key holds propagated bounds
     unsigned char* qmark;  // block proposal: on a unit block's first slot, 1 when round 2 must refresh the block
+    unsigned char* chunk_stale;  // block proposal: per leaf chunk, 1 when it holds a stale slot (set by the tree)
     // persistent kernel (persist.cuh): its grid barrier, the time limit of a
     // wait in nanoseconds, and extra arrivals a barrier waits for (0; 1 only
     // in the test that makes every wait run out)

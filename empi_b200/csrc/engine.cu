@@ -330,7 +330,7 @@ struct empi_batch {
     DevBuf<float> d_dump, d_prop, d_pscores;
     DevBuf<double> d_probe;
     DevBuf<int2> d_prange, d_qrange;
-    DevBuf<unsigned char> d_stale, d_qmark;
+    DevBuf<unsigned char> d_stale, d_qmark, d_chunk_stale;
     int prop_source = -1;  // block proposal: 0 learned network, 1 last-atom heuristic, 2 none (k = 0)
     ProposalNet net;       // the learned proposer's device weights and activations
     DevBuf<float> d_pairs; // training-pair collection: [instance][iteration][64 x 128] spectrograms
@@ -1150,6 +1150,7 @@ extern "C" empi_status empi_batch_set_proposal(empi_batch* b, int source, int k,
         b->dev.qrange = nullptr;
         b->dev.stale = nullptr;
         b->dev.qmark = nullptr;
+        b->dev.chunk_stale = nullptr;
         return ok();
     }
     if (source == 0) {
@@ -1173,6 +1174,9 @@ extern "C" empi_status empi_batch_set_proposal(empi_batch* b, int source, int k,
     if (!b->d_qmark.p) CUDA_TRY(b->d_qmark.alloc(b->d_slots.n));
     CUDA_TRY(cudaMemset(b->d_qmark.p, 0, b->d_qmark.n));
     b->dev.qmark = b->d_qmark.p;
+    if (!b->d_chunk_stale.p) CUDA_TRY(b->d_chunk_stale.alloc(b->d_chunks.n));
+    CUDA_TRY(cudaMemset(b->d_chunk_stale.p, 0, b->d_chunk_stale.n));
+    b->dev.chunk_stale = b->d_chunk_stale.p;
     return ok();
 }
 

@@ -317,6 +317,13 @@ __device__ __forceinline__ void tree_chunk(const BatchDev& b, int inst, int rem,
         best = key > best ? key : best;
         bestl = max(bestl, (unsigned)(v & 0xffffffffull));
     }
+    if (b.chunk_stale) {
+        // with a block proposal: does the chunk hold a stale slot (k_qualify's filter)
+        int any = 0;
+        for (long long s = s0 + lane; s < s1; s += 32) any |= b.stale[ip.slot_off + s];
+        any = __any_sync(0xffffffffu, any);
+        if (lane == 0) b.chunk_stale[ip.chunk_off + chunk] = (unsigned char)(any != 0);
+    }
 #pragma unroll
     for (int off = 16; off; off >>= 1) {
         unsigned long long o = __shfl_down_sync(0xffffffffu, best, off);
@@ -516,35 +523,71 @@ EMPI_GLOBAL void k_topk_ranges(BatchDev b) {
     }
 }
 
-// the bound increment of a window of scale sp at t from the instance's last atom
-__device__ __forceinline__ double atom_increment(const BatchDev& b, const InstPlan& ip, const DictPlan& dp,
-                                                 const ScalePlan& sp, const InstState& st, int t) {
+// The last atom of an instance, for the bound increment of its windows:
+// its amplitude over channels |a| = sqrt(sum_c a_c^2), centre and scale in
+// seconds; one warp, lanes over channels (any count).
+struct LastAtom {
+    double a, tA, sA;
+};
+
+__device__ __forceinline__ LastAtom last_atom_warp(const BatchDev& b, const InstPlan& ip, const DictPlan& dp,
+                                                  const InstState& st, int lane) {
     const double* p = b.atoms + ip.out_off + (long long)(st.it - 1) * ip.C * 6;
     double a2 = 0.0;
-    for (int c = 0; c < ip.C; ++c) a2 += p[c * 6 + 1] * p[c * 6 + 1];
-    const double tA = p[2] / dp.fs, sA = p[3] / dp.fs;
-    const double dt = grid_t(t, dp.tMax, sp.tcount) - tA;
-    const double w2 = sA * sA + sp.s * sp.s;
-    const double ov = dp.fs * sA * sp.s / sqrt(w2) * exp(-CUDART_PI * dt * dt / w2) + 1.0;
-    return sqrt((double)sp.Kc * (double)fmaxf(1.0f, sp.bnd_rho)) * sqrt(a2) * ov * (1.0 + 1e-6);
+    for (int c = lane; c < ip.C; c += 32) a2 += p[c * 6 + 1] * p[c * 6 + 1];
+#pragma unroll
+    for (int off = 16; off; off >>= 1) a2 += __shfl_xor_sync(0xffffffffu, a2, off);
+    return LastAtom{sqrt(a2), p[2] / dp.fs, p[3] / dp.fs};
+}
+
+// the bound increment of a window of scale sp at t from the instance's last
+// atom: |delta X| <= sqrt(Kc rho) |a| (fs sA s / sqrt(sA^2 + s^2)
+// exp(-pi dt^2 / (sA^2 + s^2)) + 1) (Gaussian overlap of atom and window)
+__device__ __forceinline__ double atom_increment(const DictPlan& dp, const ScalePlan& sp, const LastAtom& la, int t) {
+    const double dt = grid_t(t, dp.tMax, sp.tcount) - la.tA;
+    const double w2 = la.sA * la.sA + sp.s * sp.s;
+    const double ov = dp.fs * la.sA * sp.s / sqrt(w2) * exp(-CUDART_PI * dt * dt / w2) + 1.0;
+    return sqrt((double)sp.Kc * (double)fmaxf(1.0f, sp.bnd_rho)) * la.a * ov * (1.0 + 1e-6);
 }
 
 __device__ __forceinline__ bool in_range(int2 r, int t) { return t >= r.x && t <= r.y; }
 
+// Every dirty slot outside the proposed range gets bounds propagated through
+// the subtraction and is marked stale (warp per dirty leaf chunk, the atom's
+// terms once per warp).
 EMPI_GLOBAL void k_propagate_stale(BatchDev b) {
-    for_dirty_slots(b, [&](int inst, const InstPlan& ip, const DictPlan& dp, const ScalePlan& sp, int j, long long s) {
+    const int lane = threadIdx.x & 31;
+    const int total = b.ctr[CTR_TOTAL_CHUNKS];
+    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int item = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); item < total; item += nwarps) {
+        const int inst = upper_index(b.inst_chunks, b.ninst, item);
         const InstState& st = b.state[inst];
-        const int t = (int)((s - sp.slot_base) / sp.G);
-        if (st.it < 1 || in_range(b.prange[ip.ij_off + j], t)) return;  // refreshed in round 1
-        const double d = atom_increment(b, ip, dp, sp, st, t);
-        const unsigned long long key = b.slots[ip.slot_off + s];
-        const double u = sqrt((double)__uint_as_float((unsigned)(key >> 32))) + d;
-        const double l = sqrt((double)__uint_as_float((unsigned)(key & 0xffffffffull))) - d;
-        const float U = __double2float_ru(fmin(u * u, 3.0e38));
-        const float L = l > 0.0 ? __double2float_rd(l * l) : 0.0f;
-        b.slots[ip.slot_off + s] = ((unsigned long long)__float_as_uint(U) << 32) | __float_as_uint(L);
-        b.stale[ip.slot_off + s] = 1;
-    });
+        if (st.it < 1) continue;
+        int rem = item - b.inst_chunks[inst];
+        const InstPlan ip = b.insts[inst];
+        const DictPlan dp = b.dicts[ip.dict];
+        const int j = upper_index(b.ij_chunks + ip.ij_off + inst, dp.nscales, rem);
+        rem -= b.ij_chunks[ip.ij_off + inst + j];
+        const int chunk = b.ij_crange[ip.ij_off + j].x + rem;
+        const ScalePlan sp = b.scales[dp.scale0 + j];
+        const int2 dr = b.dirty[ip.ij_off + j];
+        const int2 pr = b.prange[ip.ij_off + j];
+        const LastAtom la = last_atom_warp(b, ip, dp, st, lane);
+        const long long s0 = max((long long)chunk * kChunk, sp.slot_base + (long long)dr.x * sp.G);
+        const long long s1 = min((long long)(chunk + 1) * kChunk, sp.slot_base + (long long)(dr.y + 1) * sp.G);
+        for (long long s = s0 + lane; s < s1; s += 32) {
+            const int t = (int)((s - sp.slot_base) / sp.G);
+            if (in_range(pr, t)) continue;  // refreshed in round 1
+            const double d = atom_increment(dp, sp, la, t);
+            const unsigned long long key = b.slots[ip.slot_off + s];
+            const double u = sqrt((double)__uint_as_float((unsigned)(key >> 32))) + d;
+            const double l = sqrt((double)__uint_as_float((unsigned)(key & 0xffffffffull))) - d;
+            const float U = __double2float_ru(fmin(u * u, 3.0e38));
+            const float L = l > 0.0 ? __double2float_rd(l * l) : 0.0f;
+            b.slots[ip.slot_off + s] = ((unsigned long long)__float_as_uint(U) << 32) | __float_as_uint(L);
+            b.stale[ip.slot_off + s] = 1;
+        }
+    }
 }
 
 // per instance: the largest certified lower bound of any slot after round 1
@@ -582,7 +625,7 @@ EMPI_GLOBAL void k_qualify(BatchDev b, int total_chunks) {
         const InstPlan ip = b.insts[inst];
         const unsigned lb = st.lround;
         const int c = item - (int)ip.chunk_off;
-        if ((unsigned)(b.chunks[item] >> 32) < lb) continue;
+        if (!b.chunk_stale[item] || (unsigned)(b.chunks[item] >> 32) < lb) continue;
         const DictPlan dp = b.dicts[ip.dict];
         const long long s0 = (long long)c * kChunk;
         const long long s1 = min(s0 + kChunk, dp.slots);
