@@ -796,18 +796,29 @@ __device__ __forceinline__ void cand_slots_inst(const BatchDev& b, int inst) {
         if ((unsigned)(b.chunks[ip.chunk_off + c] >> 32) < tbits) continue;
         const long long s0 = (long long)c * kChunk;
         const long long s1 = min(s0 + kChunk, dp.slots);
-        for (long long s = s0 + lane; s < s1; s += 32) {
-            const unsigned long long v = b.slots[ip.slot_off + s];
-            if ((unsigned)(v >> 32) >= tbits) {
-                atomicMax(&s_tstar, (unsigned)(v & 0xffffffffull));
-                const int at = atomicAdd(b.ctr + CTR_CSLOTS, 1);
-                if (at < b.cslot_cap) {
-                    CandSlot cs;
-                    cs.inst = inst;
-                    slot_to_jtg(b, dp, s, cs.j, cs.t, cs.g);
-                    b.cslots[at] = cs;
-                } else {
-                    st.err = ERR_CAND_OVERFLOW;
+        // a lane's kChunk / 32 slots in batches of kScanBatch independent loads:
+        // the warp scans a chunk in a few L2 round trips, not one per slot
+        constexpr int kScanBatch = 8;
+        for (long long sb = s0 + lane; sb < s1; sb += 32 * kScanBatch) {
+            unsigned long long v[kScanBatch];
+#pragma unroll
+            for (int i = 0; i < kScanBatch; ++i) {
+                const long long s = sb + 32 * i;
+                v[i] = s < s1 ? b.slots[ip.slot_off + s] : 0ull;
+            }
+#pragma unroll
+            for (int i = 0; i < kScanBatch; ++i) {
+                if (sb + 32 * i < s1 && (unsigned)(v[i] >> 32) >= tbits) {
+                    atomicMax(&s_tstar, (unsigned)(v[i] & 0xffffffffull));
+                    const int at = atomicAdd(b.ctr + CTR_CSLOTS, 1);
+                    if (at < b.cslot_cap) {
+                        CandSlot cs;
+                        cs.inst = inst;
+                        slot_to_jtg(b, dp, sb + 32 * i, cs.j, cs.t, cs.g);
+                        b.cslots[at] = cs;
+                    } else {
+                        st.err = ERR_CAND_OVERFLOW;
+                    }
                 }
             }
         }
