@@ -316,6 +316,16 @@ struct empi_batch {
     cudaStream_t copy_stream = nullptr;  // staged loads of the next batch (batch_stage)
     cudaEvent_t staged_ev = nullptr;
     bool staged = false;
+    // host copy of the last run's results (per-instance state, energies,
+    // indices, atoms, MMP2 channel fits), filled by a few bulk copies on the
+    // first read after a run (fetch_results) instead of several small copies
+    // per epoch and channel; invalid from the next load or run on
+    struct {
+        bool valid = false;
+        std::vector<InstState> st;
+        std::vector<double> en, atoms, fit;
+        std::vector<int4> ind;
+    } hm;
     DevBuf<WinGeom> d_wgeom;
     DevBuf<double> d_residual, d_atoms, d_energies, d_chan_energy, d_fit_atoms, d_stats;
     DevBuf<InstState> d_state;
@@ -924,12 +934,14 @@ extern "C" empi_status empi_batch_load(empi_batch* b, const empi_epoch* epochs) 
     }
     CUDA_TRY(cudaStreamSynchronize(b->eng->stream));
     b->staged = false;  // these epochs replace any staged ones
+    b->hm.valid = false;
     return ok();
 }
 
 namespace empi {
 
 empi_status batch_load_device(empi_batch* b, const float* const* device_data) {
+    b->hm.valid = false;
     for (size_t e = 0; e < b->epochs.size(); ++e)
         CUDA_TRY(cudaMemcpyAsync(b->d_input.p + b->epoch_in_off[e], device_data[e],
                                  sizeof(float) * (size_t)b->epochs[e].channels * b->epochs[e].samples,
@@ -986,6 +998,7 @@ empi_status batch_run_hooked(empi_batch* b, const std::function<void()>& after_c
     if (!b) return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
     empi_status st = set_device(b->eng);
     if (st != EMPI_OK) return st;
+    b->hm.valid = false;
     st = capture_graph(b);
     if (st != EMPI_OK) return st;
     cudaStream_t s = b->eng->stream;
@@ -1320,34 +1333,57 @@ extern "C" empi_status empi_batch_probe_proposal(empi_batch* b, int enable) {
     return ok();
 }
 
+namespace {
+
+// the last run's results on the host, copied once per run (empi_batch_atoms
+// and empi_batch_total_energy read every epoch from this copy)
+empi_status fetch_results(empi_batch* b) {
+    if (b->hm.valid) return EMPI_OK;
+    auto& h = b->hm;
+    h.st.resize(b->insts.size());
+    h.en.resize(b->d_energies.n);
+    h.ind.resize(b->d_indices.n);
+    h.atoms.resize(b->d_atoms.n);
+    h.fit.resize(b->d_fit_atoms.n);
+    CUDA_TRY(cudaMemcpy(h.st.data(), b->d_state.p, sizeof(InstState) * h.st.size(), cudaMemcpyDeviceToHost));
+    if (!h.en.empty())
+        CUDA_TRY(cudaMemcpy(h.en.data(), b->d_energies.p, sizeof(double) * h.en.size(), cudaMemcpyDeviceToHost));
+    if (!h.ind.empty())
+        CUDA_TRY(cudaMemcpy(h.ind.data(), b->d_indices.p, sizeof(int4) * h.ind.size(), cudaMemcpyDeviceToHost));
+    if (!h.atoms.empty())
+        CUDA_TRY(cudaMemcpy(h.atoms.data(), b->d_atoms.p, sizeof(double) * h.atoms.size(), cudaMemcpyDeviceToHost));
+    if (!h.fit.empty())
+        CUDA_TRY(cudaMemcpy(h.fit.data(), b->d_fit_atoms.p, sizeof(double) * h.fit.size(), cudaMemcpyDeviceToHost));
+    h.valid = true;
+    return EMPI_OK;
+}
+
+}  // namespace
+
 extern "C" empi_status empi_batch_atoms(empi_batch* b, int epoch, int cap, double* atoms, int* count,
                                         double* energies, int* indices) {
     if (!b || epoch < 0 || epoch >= (int)b->epochs.size() || cap < 0 || (cap > 0 && !atoms))
         return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
     empi_status st = set_device(b->eng);
     if (st != EMPI_OK) return st;
+    st = fetch_results(b);
+    if (st != EMPI_OK) return st;
+    const auto& h = b->hm;
     const int C = b->epochs[epoch].channels;
     const int iters = b->settings.iteration_max;
     const int i0 = b->epoch_first_inst[epoch];
     const InstPlan& ip0 = b->insts[i0];
-    const int ninst_e = (ip0.chan0 >= 0) ? C : 1;  // SMP: one loop per channel
-    std::vector<InstState> sts(ninst_e);
-    CUDA_TRY(cudaMemcpy(sts.data(), b->d_state.p + i0, sizeof(InstState) * ninst_e, cudaMemcpyDeviceToHost));
-    std::vector<double> en((size_t)ninst_e * iters);
-    std::vector<int4> ind((size_t)ninst_e * iters);
-    CUDA_TRY(cudaMemcpy(en.data(), b->d_energies.p + (size_t)i0 * iters, sizeof(double) * en.size(),
-                        cudaMemcpyDeviceToHost));
-    CUDA_TRY(cudaMemcpy(ind.data(), b->d_indices.p + (size_t)i0 * iters, sizeof(int4) * ind.size(),
-                        cudaMemcpyDeviceToHost));
+    const InstState* sts = h.st.data() + i0;
+    const double* en = h.en.data() + (size_t)i0 * iters;
+    const int4* ind = h.ind.data() + (size_t)i0 * iters;
     const int lim = std::min(cap, iters);
-    if (ip0.chan0 >= 0) {  // SMP
+    if (ip0.chan0 >= 0) {  // SMP: one loop per channel
         for (int c = 0; c < C; ++c) {
             const InstPlan& ip = b->insts[i0 + c];
             const int n = std::min(sts[c].it, lim);
             if (count) count[c] = sts[c].it;
             if (n > 0)
-                CUDA_TRY(cudaMemcpy(atoms + (size_t)c * cap * 6, b->d_atoms.p + ip.out_off, sizeof(double) * 6 * n,
-                                    cudaMemcpyDeviceToHost));
+                std::memcpy(atoms + (size_t)c * cap * 6, h.atoms.data() + ip.out_off, sizeof(double) * 6 * n);
             for (int a = 0; a < lim; ++a) {
                 if (energies) energies[(size_t)c * cap + a] = en[(size_t)c * iters + a];
                 if (indices) {
@@ -1366,17 +1402,13 @@ extern "C" empi_status empi_batch_atoms(empi_batch* b, int epoch, int cap, doubl
             const int f0 = b->epoch_first_fit[epoch];
             for (int c = 0; c < C; ++c)
                 if (n > 0)
-                    CUDA_TRY(cudaMemcpy(atoms + (size_t)c * cap * 6, b->d_fit_atoms.p + ((size_t)(f0 + c) * iters) * 6,
-                                        sizeof(double) * 6 * n, cudaMemcpyDeviceToHost));
+                    std::memcpy(atoms + (size_t)c * cap * 6, h.fit.data() + ((size_t)(f0 + c) * iters) * 6,
+                                sizeof(double) * 6 * n);
         } else {
-            std::vector<double> tmp((size_t)std::max(n, 1) * C * 6);
-            if (n > 0)
-                CUDA_TRY(cudaMemcpy(tmp.data(), b->d_atoms.p + ip0.out_off, sizeof(double) * tmp.size(),
-                                    cudaMemcpyDeviceToHost));
+            const double* src = h.atoms.data() + ip0.out_off;  // [a][c][6]
             for (int a = 0; a < n; ++a)
                 for (int c = 0; c < C; ++c)
-                    std::memcpy(atoms + ((size_t)c * cap + a) * 6, tmp.data() + ((size_t)a * C + c) * 6,
-                                sizeof(double) * 6);
+                    std::memcpy(atoms + ((size_t)c * cap + a) * 6, src + ((size_t)a * C + c) * 6, sizeof(double) * 6);
         }
         for (int a = 0; a < lim; ++a) {
             if (energies) energies[a] = en[a];
@@ -1395,11 +1427,11 @@ extern "C" empi_status empi_batch_total_energy(empi_batch* b, int epoch, double*
         return fail(EMPI_ERR_INVALID_ARGUMENT, "invalidArgument");
     empi_status st = set_device(b->eng);
     if (st != EMPI_OK) return st;
+    st = fetch_results(b);
+    if (st != EMPI_OK) return st;
     const int i0 = b->epoch_first_inst[epoch];
     const int n = b->insts[i0].chan0 >= 0 ? b->epochs[epoch].channels : 1;
-    std::vector<InstState> sts(n);
-    CUDA_TRY(cudaMemcpy(sts.data(), b->d_state.p + i0, sizeof(InstState) * n, cudaMemcpyDeviceToHost));
-    for (int i = 0; i < n; ++i) totals[i] = sts[i].etotal;
+    for (int i = 0; i < n; ++i) totals[i] = b->hm.st[i0 + i].etotal;
     return ok();
 }
 
