@@ -536,7 +536,7 @@ void launch_proposal_update(empi_batch* b, cudaStream_t s, cudaEvent_t e0, cudaE
     k_root<<<ninst, 256, 0, s>>>(b->dev);
     k_qualify<<<b->tree_grid, 256, 0, s>>>(b->dev, b->total_chunks);
     cudaMemsetAsync(b->dev.lcount, 0, sizeof(int) * 2 * 16, s);
-    k_round2_sched<<<ninst, 128, 0, s>>>(b->dev);
+    k_round2_sched<<<ninst, 512, 0, s>>>(b->dev);
     k_chunk_prefix<<<1, std::min(1024, 32 * ((ninst + 31) / 32)), 0, s>>>(b->dev);
     launch_refresh(b, s);
     if (e1) cudaEventRecord(e1, s);

@@ -629,16 +629,44 @@ EMPI_GLOBAL void k_qualify(BatchDev b, int total_chunks) {
         const DictPlan dp = b.dicts[ip.dict];
         const long long s0 = (long long)c * kChunk;
         const long long s1 = min(s0 + kChunk, dp.slots);
-        for (long long s = s0 + lane; s < s1; s += 32) {
-            if (!b.stale[ip.slot_off + s] || (unsigned)(b.slots[ip.slot_off + s] >> 32) < lb) continue;
-            int j, t, g;
-            slot_to_jtg(b, dp, s, j, t, g);
-            // mark the group's unit block holding t (on the block's first slot)
-            const ScalePlan& sp = b.scales[dp.scale0 + j];
-            const int B = g >= 2 ? sp.B2 : sp.B1;
-            b.qmark[ip.slot_off + sp.slot_base + (long long)(t / B) * B * sp.G + g] = 1;
-            atomicMin(&b.qrange[ip.ij_off + j].x, t);
-            atomicMax(&b.qrange[ip.ij_off + j].y, t);
+        // the chunk's slots, kScanBatch stale flags and keys per lane in
+        // flight; the loop runs the same trips in every lane (warp collectives
+        // below), slots past the chunk's end do not qualify
+        constexpr int kScanBatch = 8;
+        for (long long base = s0; base < s1; base += 32 * kScanBatch) {
+            unsigned char sv[kScanBatch];
+            unsigned long long kv[kScanBatch];
+#pragma unroll
+            for (int i = 0; i < kScanBatch; ++i) {
+                const long long s = base + lane + 32 * i;
+                sv[i] = s < s1 ? b.stale[ip.slot_off + s] : 0;
+                kv[i] = s < s1 ? b.slots[ip.slot_off + s] : 0ull;
+            }
+#pragma unroll
+            for (int i = 0; i < kScanBatch; ++i) {
+                const long long s = base + lane + 32 * i;
+                const bool q = sv[i] && (unsigned)(kv[i] >> 32) >= lb;
+                if (!__any_sync(0xffffffffu, q)) continue;
+                int j = -1, t = 0;
+                if (q) {
+                    int g;
+                    slot_to_jtg(b, dp, s, j, t, g);
+                    // mark the group's unit block holding t (on the block's first slot)
+                    const ScalePlan& sp = b.scales[dp.scale0 + j];
+                    const int B = g >= 2 ? sp.B2 : sp.B1;
+                    b.qmark[ip.slot_off + sp.slot_base + (long long)(t / B) * B * sp.G + g] = 1;
+                }
+                // the scale's t range: one atomic pair per scale present in the
+                // warp's qualifying slots, not one per slot
+                const unsigned grp = __match_any_sync(0xffffffffu, j);
+                if (q) {
+                    const int tmin = __reduce_min_sync(grp, t), tmax = __reduce_max_sync(grp, t);
+                    if (lane == __ffs(grp) - 1) {
+                        atomicMin(&b.qrange[ip.ij_off + j].x, tmin);
+                        atomicMax(&b.qrange[ip.ij_off + j].y, tmax);
+                    }
+                }
+            }
         }
     }
 }
@@ -662,10 +690,15 @@ EMPI_GLOBAL void k_round2_sched(BatchDev b) {
     const int inst = blockIdx.x;
     const InstPlan ip = b.insts[inst];
     const DictPlan dp = b.dicts[ip.dict];
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     double st_flops = 0.0, st_bytes = 0.0, st_slots = 0.0;
-    for (int j = threadIdx.x; j < dp.nscales; j += blockDim.x) {
+    // a warp per scale, its lanes over 32 consecutive unit blocks at a time
+    // (the marks of a wide range are read in parallel, and a warp takes its
+    // units' list places with one atomic per round)
+    for (int j = threadIdx.x >> 5; j < dp.nscales; j += nw) {
         const int2 q = b.qrange[ip.ij_off + j];
-        b.qrange[ip.ij_off + j] = make_int2(0x7fffffff, -1);
+        __syncwarp();
+        if (lane == 0) b.qrange[ip.ij_off + j] = make_int2(0x7fffffff, -1);
         if (q.y < q.x) continue;
         const ScalePlan sp = b.scales[dp.scale0 + j];
         const int cap = b.lcap[sp.logL];
@@ -673,19 +706,31 @@ EMPI_GLOBAL void k_round2_sched(BatchDev b) {
         int tmin = 0x7fffffff, tmax = -1;
         for (int g = 0; g < sp.G; ++g) {
             const int B = g >= 2 ? sp.B2 : sp.B1;
-            for (int t0 = (q.x / B) * B; t0 <= q.y; t0 += B) {
-                unsigned char* mk = b.qmark + ip.slot_off + sp.slot_base + (long long)t0 * sp.G + g;
-                if (!*mk) continue;
-                *mk = 0;
-                const int n = min(B, sp.tcount - t0);
-                const int at = atomicAdd(b.lcount + sp.logL, 1);
-                if (at < cap) list[at] = make_int4(inst, j | (g << 16), t0, n);
-                refresh_stats_group(dp, sp, ip.C, g, t0, t0 + n - 1, st_flops, st_bytes, st_slots);
-                tmin = min(tmin, t0);
-                tmax = max(tmax, t0 + n - 1);
+            for (int first = (q.x / B) * B; first <= q.y; first += 32 * B) {
+                const int t0 = first + lane * B;
+                bool emit = false;
+                if (t0 <= q.y) {
+                    unsigned char* mk = b.qmark + ip.slot_off + sp.slot_base + (long long)t0 * sp.G + g;
+                    emit = *mk != 0;
+                    if (emit) *mk = 0;
+                }
+                const unsigned em = __ballot_sync(0xffffffffu, emit);
+                if (!em) continue;
+                int at = 0;
+                if (lane == 0) at = atomicAdd(b.lcount + sp.logL, __popc(em));
+                at = __shfl_sync(0xffffffffu, at, 0) + __popc(em & ((1u << lane) - 1u));
+                if (emit) {
+                    const int n = min(B, sp.tcount - t0);
+                    if (at < cap) list[at] = make_int4(inst, j | (g << 16), t0, n);
+                    refresh_stats_group(dp, sp, ip.C, g, t0, t0 + n - 1, st_flops, st_bytes, st_slots);
+                    tmin = min(tmin, t0);
+                    tmax = max(tmax, t0 + n - 1);
+                }
             }
         }
-        if (tmax < tmin) continue;
+        tmin = __reduce_min_sync(0xffffffffu, tmin);
+        tmax = __reduce_max_sync(0xffffffffu, tmax);
+        if (tmax < tmin || lane != 0) continue;
         // the leaf chunks the tree re-reduces after round 2: the dirty range's
         // and the refreshed blocks' (stale slots of earlier iterations lie
         // outside the dirty range), as one covering range
@@ -698,7 +743,14 @@ EMPI_GLOBAL void k_round2_sched(BatchDev b) {
         }
         b.ij_crange[ip.ij_off + j] = make_int2(c0, c1 - c0 + 1);
     }
-    if (st_flops != 0.0) {
+    // the work statistics: summed over the warp, one set of atomics per warp
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+        st_flops += __shfl_down_sync(0xffffffffu, st_flops, off);
+        st_bytes += __shfl_down_sync(0xffffffffu, st_bytes, off);
+        st_slots += __shfl_down_sync(0xffffffffu, st_slots, off);
+    }
+    if (lane == 0 && st_flops != 0.0) {
         atomicAdd(b.stats + 0, st_flops);
         atomicAdd(b.stats + 1, st_bytes);
         atomicAdd(b.stats + 2, st_slots);
