@@ -575,17 +575,25 @@ EMPI_GLOBAL void k_propagate_stale(BatchDev b) {
         const LastAtom la = last_atom_warp(b, ip, dp, st, lane);
         const long long s0 = max((long long)chunk * kChunk, sp.slot_base + (long long)dr.x * sp.G);
         const long long s1 = min((long long)(chunk + 1) * kChunk, sp.slot_base + (long long)(dr.y + 1) * sp.G);
-        for (long long s = s0 + lane; s < s1; s += 32) {
-            const int t = (int)((s - sp.slot_base) / sp.G);
+        if (s0 >= s1) continue;
+        // a lane per window of the chunk: the increment once per window, then
+        // the window's residue-group slots that lie in the chunk
+        const int t0 = (int)((s0 - sp.slot_base) / sp.G), t1 = (int)((s1 - 1 - sp.slot_base) / sp.G);
+        for (int t = t0 + lane; t <= t1; t += 32) {
             if (in_range(pr, t)) continue;  // refreshed in round 1
             const double d = atom_increment(dp, sp, la, t);
-            const unsigned long long key = b.slots[ip.slot_off + s];
-            const double u = sqrt((double)__uint_as_float((unsigned)(key >> 32))) + d;
-            const double l = sqrt((double)__uint_as_float((unsigned)(key & 0xffffffffull))) - d;
-            const float U = __double2float_ru(fmin(u * u, 3.0e38));
-            const float L = l > 0.0 ? __double2float_rd(l * l) : 0.0f;
-            b.slots[ip.slot_off + s] = ((unsigned long long)__float_as_uint(U) << 32) | __float_as_uint(L);
-            b.stale[ip.slot_off + s] = 1;
+            const long long sw = sp.slot_base + (long long)t * sp.G;
+            for (int g = 0; g < sp.G; ++g) {
+                const long long s = sw + g;
+                if (s < s0 || s >= s1) continue;
+                const unsigned long long key = b.slots[ip.slot_off + s];
+                const double u = sqrt((double)__uint_as_float((unsigned)(key >> 32))) + d;
+                const double l = sqrt((double)__uint_as_float((unsigned)(key & 0xffffffffull))) - d;
+                const float U = __double2float_ru(fmin(u * u, 3.0e38));
+                const float L = l > 0.0 ? __double2float_rd(l * l) : 0.0f;
+                b.slots[ip.slot_off + s] = ((unsigned long long)__float_as_uint(U) << 32) | __float_as_uint(L);
+                b.stale[ip.slot_off + s] = 1;
+            }
         }
     }
 }
@@ -633,6 +641,10 @@ EMPI_GLOBAL void k_qualify(BatchDev b, int total_chunks) {
         // flight; the loop runs the same trips in every lane (warp collectives
         // below), slots past the chunk's end do not qualify
         constexpr int kScanBatch = 8;
+        // the scale of the chunk's first slot; later slots of the chunk step
+        // forward from it (a chunk spans few scales)
+        int jc, tfirst, gfirst;
+        slot_to_jtg(b, dp, s0, jc, tfirst, gfirst);
         for (long long base = s0; base < s1; base += 32 * kScanBatch) {
             unsigned char sv[kScanBatch];
             unsigned long long kv[kScanBatch];
@@ -649,10 +661,13 @@ EMPI_GLOBAL void k_qualify(BatchDev b, int total_chunks) {
                 if (!__any_sync(0xffffffffu, q)) continue;
                 int j = -1, t = 0;
                 if (q) {
-                    int g;
-                    slot_to_jtg(b, dp, s, j, t, g);
-                    // mark the group's unit block holding t (on the block's first slot)
+                    j = jc;
+                    while (j + 1 < dp.nscales && b.scales[dp.scale0 + j + 1].slot_base <= s) ++j;
                     const ScalePlan& sp = b.scales[dp.scale0 + j];
+                    const int rel = (int)(s - sp.slot_base);
+                    t = rel / sp.G;
+                    const int g = rel - t * sp.G;
+                    // mark the group's unit block holding t (on the block's first slot)
                     const int B = g >= 2 ? sp.B2 : sp.B1;
                     b.qmark[ip.slot_off + sp.slot_base + (long long)(t / B) * B * sp.G + g] = 1;
                 }
