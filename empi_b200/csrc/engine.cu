@@ -523,14 +523,17 @@ empi_status net_load(empi_batch* b, const char* path) {
 // bounds, round 2 refreshes those still reaching the root's lower bound
 void launch_proposal_update(empi_batch* b, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
     const int ninst = (int)b->insts.size();
+    // without a proposer (source 2, k = 0) no block is proposed: the proposed
+    // ranges stay empty and round 1 has no unit, so neither runs
+    const bool round1 = b->prop_source != 2;
     if (b->prop_source == 1) k_scores_last_atom<<<ninst, 256, 0, s>>>(b->dev);
     else if (b->prop_source == 0) launch_net(b, s);
-    k_topk_ranges<<<ninst, 256, 0, s>>>(b->dev);
+    if (round1) k_topk_ranges<<<ninst, 256, 0, s>>>(b->dev);
     cudaMemsetAsync(b->dev.lcount, 0, sizeof(int) * 2 * 16, s);
     k_sched_a<<<ninst, 128, 0, s>>>(b->dev, SCHED_ITERATE, -1, 0.0, 0.0);
     k_sched_b<<<1, std::min(1024, 32 * ((ninst + 31) / 32)), 0, s>>>(b->dev);
     if (e0) cudaEventRecord(e0, s);
-    launch_refresh(b, s);
+    if (round1) launch_refresh(b, s);
     k_propagate_stale<<<b->tree_grid, 256, 0, s>>>(b->dev);
     k_tree<<<b->tree_grid, 256, 0, s>>>(b->dev);
     k_root<<<ninst, 256, 0, s>>>(b->dev);
