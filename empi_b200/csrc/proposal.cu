@@ -30,7 +30,15 @@ __device__ __forceinline__ float* spec_at(float* out, const InstState& st, int i
     return out + (long long)inst * inst_stride + (per_it ? (long long)st.it * kSpecSize : 0);
 }
 
+// One CTA per (frame, instance), a thread per bin.  The frame's Hann-windowed
+// samples are staged in shared memory kSpecStage at a time (the window once
+// per sample, not once per bin and sample); each bin's twiddle e^{-2 pi i nu m}
+// is rotated from sample to sample and set exactly at every stage's start,
+// so the rotation's rounding stays at the 1e-5 level of a heuristic input.
+constexpr int kSpecStage = 256;
+
 __global__ void k_spectrogram(BatchDev b, float* out, long long inst_stride, int per_it) {
+    __shared__ float sv[kSpecStage];
     const int inst = blockIdx.y, frame = blockIdx.x, k = threadIdx.x;
     const InstState& st = b.state[inst];
     if (st.status != ST_RUNNING || (per_it && st.it >= b.iter_max)) return;
@@ -40,20 +48,32 @@ __global__ void k_spectrogram(BatchDev b, float* out, long long inst_stride, int
     const int Wf = max(4, 2 * ((N + kSpecT - 1) / kSpecT));
     const int c0 = (int)(((long long)(2 * frame + 1) * N) / (2 * kSpecT));
     const int n0 = c0 - Wf / 2;
-    float pw = 0.0f;
     const float nu = (k + 0.5f) / (2.0f * kSpecF);  // cycles per sample
+    float stp_s, stp_c;
+    sincospif(-2.0f * nu, &stp_s, &stp_c);
+    const float2 step = make_float2(stp_c, stp_s);
+    float pw = 0.0f;
     for (int c = 0; c < ip.C; ++c) {
         const float* x = b.residual32 + ip.res_off + (long long)c * N;
         float ar = 0.0f, ai = 0.0f;
-        for (int m = 0; m < Wf; ++m) {
-            const int n = n0 + m;
-            if (n < 0 || n >= N) continue;
-            float s, co;
-            sincospif(-2.0f * nu * (float)m, &s, &co);
-            const float w = 0.5f - 0.5f * cospif(2.0f * (m + 0.5f) / (float)Wf);
-            const float v = x[n] * w;
-            ar += v * co;
-            ai += v * s;
+        for (int m0 = 0; m0 < Wf; m0 += kSpecStage) {
+            const int len = min(kSpecStage, Wf - m0);
+            __syncthreads();  // the previous stage's samples are consumed
+            for (int i = k; i < len; i += blockDim.x) {
+                const int m = m0 + i, n = n0 + m;
+                const float w = 0.5f - 0.5f * cospif(2.0f * (m + 0.5f) / (float)Wf);
+                sv[i] = (n >= 0 && n < N) ? x[n] * w : 0.0f;
+            }
+            __syncthreads();
+            float ts, tc;
+            sincospif(-2.0f * nu * (float)m0, &ts, &tc);
+            float2 t = make_float2(tc, ts);
+            for (int i = 0; i < len; ++i) {
+                const float v = sv[i];
+                ar += v * t.x;
+                ai += v * t.y;
+                t = make_float2(t.x * step.x - t.y * step.y, t.x * step.y + t.y * step.x);
+            }
         }
         pw += ar * ar + ai * ai;
     }
