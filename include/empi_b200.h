@@ -229,7 +229,11 @@ empi_status empi_batch_run(empi_batch* batch);
  * the atom count per channel.  energies (optional): residual energy after
  * each iteration of the loop that produced the channel's atoms
  * ([channel][cap] for SMP, [cap] otherwise; NaN where none was computed).
- * indices (optional): (scale, t, f) per atom, same layout as energies x 3. */
+ * indices (optional): (scale, t, f) per atom, same layout as energies x 3.
+ * The first read after a run copies the whole batch's results to the host in
+ * a few bulk copies; later reads of any epoch (this call and
+ * empi_batch_total_energy) are served from that copy until the next load or
+ * run. */
 empi_status empi_batch_atoms(empi_batch* batch, int epoch, int cap, double* atoms, int* count,
                              double* energies, int* indices);
 
