@@ -171,6 +171,36 @@ def test_batch_rerun_is_deterministic(engine):
     b.close()
 
 
+@pytest.mark.parametrize("variant", ["smp", "mmp2", "mmp3"])
+def test_results_follow_each_load_and_run(engine, variant):
+    """A batch's results are read from one host copy per run: after new
+    epochs are loaded and run, every read (atoms, energies, indices, totals)
+    gives the new run's results, equal to a fresh batch's on those epochs."""
+    from empi_b200 import synth
+
+    wa = synth.workload(1, epochs=2, channels=3, samples=1024, seed=91)
+    wb = synth.workload(1, epochs=2, channels=3, samples=1024, seed=92)
+    settings = empi_b200.DecompositionSettings(12, 0.0)
+    shapes = [e.shape for e in wa.epochs]
+    b = empi_b200.Batch(variant, 0.01, settings, shapes, wa.fs, engine=engine)
+    b.load(wa.epochs)
+    b.run()
+    ra = [b.result(e) for e in range(2)]
+    b.load(wb.epochs)
+    b.run()
+    rb = [b.result(e) for e in range(2)]
+    b.close()
+    fresh = empi_b200.Batch(variant, 0.01, settings, shapes, wb.fs, engine=engine)
+    fresh.load(wb.epochs)
+    fresh.run()
+    rf = [fresh.result(e) for e in range(2)]
+    fresh.close()
+    for x, y, z in zip(ra, rb, rf):
+        assert not np.array_equal(x.atoms, y.atoms)
+        for field in ("atoms", "counts", "energies", "indices", "totals"):
+            assert np.array_equal(getattr(y, field), getattr(z, field), equal_nan=field == "energies"), field
+
+
 def decode_book(data):
     """Minimal MPv5 decoder (field conversions of the reference's utils/readbook.cpp)."""
     import struct
